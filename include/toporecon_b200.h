@@ -1,0 +1,166 @@
+/*
+ * toporecon_b200 -- C ABI of the Blackwell (sm_100a) backend for toporecon's
+ * PDHG reconstruction loop (TVM / TVME / TVMW).
+ *
+ * Reference interfaces replaced (paths inside MRI-Research/MultiNodeMRI-MICCAI26):
+ *   NufftBackend contract ............ src/toporecon/nufft_backend.py:11-52
+ *   SigPyNufftBackend.__init__ ....... src/toporecon/nufft_backend.py:58-88
+ *   SigPyNufftBackend.forward ........ src/toporecon/nufft_backend.py:101-107
+ *   SigPyNufftBackend.adjoint ........ src/toporecon/nufft_backend.py:109-116
+ *   data dual step (b,c,e loop) ...... src/toporecon/algorithms/tvme.py:256-267
+ *   coil-combined adjoint ............ src/toporecon/algorithms/tvme.py:382-394
+ *   TvmReconstructor.pdhg ............ src/toporecon/algorithms/tvm.py:227-380
+ *   TvmeReconstructor.pdhg ........... src/toporecon/algorithms/tvme.py:208-482
+ *   TvmwReconstructor.pdhg ........... src/toporecon/algorithms/tvmw.py:385-685
+ *   *Reconstructor.run tolerance ..... src/toporecon/algorithms/tvme.py:512-557,
+ *                                      tvm.py:406-472, tvmw.py:716-773
+ *
+ * Conventions
+ *   - Complex data are interleaved float pairs (numpy complex64 / torch.cfloat).
+ *   - Images are C-order (..., Z, Y, X); coordinates are (M, 3) ordered z, y, x
+ *     in grid units (the reference's internal convention, nufft_backend.py:14-16).
+ *   - Every entry point returns a tr_status; none aborts or throws.  The text of
+ *     the last failure on the calling thread is returned by tr_last_error_string.
+ *   - Device pointers belong to the caller.  A plan owns only its sorted copy of
+ *     the trajectory, its permutation and tile tables, its coil maps and its
+ *     FFT/gridding workspace, all freed by tr_plan_destroy.
+ *   - All work is enqueued on the caller's stream (cudaStream_t passed as void*);
+ *     a plan is used by one stream at a time.
+ */
+#ifndef TOPORECON_B200_H
+#define TOPORECON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t tr_status;
+#define TR_OK 0
+#define TR_ERR_INVALID_ARG 1  /* bad shape, pointer, bin index (reference: ValueError / IndexError) */
+#define TR_ERR_OOM 2          /* device allocation failed */
+#define TR_ERR_NONFINITE 3    /* a tolerance reduction saw NaN/Inf */
+#define TR_ERR_TIMEOUT 4      /* a bounded device-side wait expired */
+#define TR_ERR_CUDA 5         /* any other CUDA runtime failure */
+#define TR_ERR_UNSUPPORTED 6  /* legal but unsupported configuration */
+
+#define TR_ALG_TVM 0
+#define TR_ALG_TVME 1
+#define TR_ALG_TVMW 2
+
+typedef struct tr_plan tr_plan;
+
+/* Plan description (replaces SigPyNufftBackend(img_shape, coordinates, device),
+ * nufft_backend.py:58-88, for every local motion bin at once). */
+typedef struct {
+    int32_t img_shape[3];        /* Z, Y, X; each >= 10 */
+    int32_t n_bins;              /* >= 1 */
+    const int64_t* bin_counts;   /* host [n_bins]: samples per bin (TR_b * RO) */
+    const float* coords;         /* host [sum(bin_counts) * 3]: zyx grid units, bins concatenated */
+    const float* dcf;            /* host [sum(bin_counts)] density weights, or NULL (all ones) */
+    int32_t n_coils;             /* C >= 1 (columns per echo on the batched path) */
+    int32_t n_echoes;            /* E >= 1 */
+    float oversamp;              /* must be 1.25 (SigPy default used by the reference) */
+    int32_t width;               /* must be 4 (SigPy default used by the reference) */
+    int32_t device;              /* CUDA device ordinal */
+    int32_t flags;               /* TR_PLAN_* bits */
+} tr_plan_desc;
+
+#define TR_PLAN_AUTOTUNE 1       /* time candidate launch shapes at plan creation */
+
+typedef struct {
+    int32_t os_shape[3];         /* oversampled grid (ceil(1.25 n) per axis) */
+    int64_t total_samples;
+    int64_t workspace_bytes;     /* device bytes owned by the plan */
+    int32_t wavelet_levels;      /* db6 levels for TVMW (PyWavelets max level) */
+    int64_t wavelet_coeffs;      /* db6 coefficients per (bin, echo) image */
+    int32_t fft_line_width;      /* columns per CTA chosen for the FFT passes */
+} tr_plan_info_t;
+
+tr_status tr_plan_create(const tr_plan_desc* desc, tr_plan** out);
+tr_status tr_plan_destroy(tr_plan* plan);
+tr_status tr_plan_info(const tr_plan* plan, tr_plan_info_t* info);
+const char* tr_last_error_string(void);
+
+/* Coil sensitivities (C, Z, Y, X) complex64 on the device; copied into the
+ * plan's coil-interleaved layout.  Needed by the batched path only. */
+tr_status tr_plan_set_maps(tr_plan* plan, const void* mps, void* stream);
+
+/* Sample order conversion for one bin.
+ * External: (ncol, M_b) acquisition order (the reference's per-bin (E, C, TR_b, RO)).
+ * Internal: (M_b, ncol) tile-sorted, columns interleaved. */
+tr_status tr_plan_sort_kspace(tr_plan* plan, int32_t bin, const void* ext, void* internal,
+                              int32_t ncol, void* stream);
+tr_status tr_plan_unsort_kspace(tr_plan* plan, int32_t bin, const void* internal, void* ext,
+                                int32_t ncol, void* stream);
+
+/* Drop-in single-image NUFFT: NufftBackend.forward(image, bin) / .adjoint(ksp, bin)
+ * (nufft_backend.py:101-116).  image (Z, Y, X), ksp (M_b) in acquisition order.
+ * The adjoint applies no density weights (the caller passes dcf*q as the
+ * reference does, tvme.py:389-391). */
+tr_status tr_nufft_forward(tr_plan* plan, int32_t bin, const void* image, void* ksp, void* stream);
+tr_status tr_nufft_adjoint(tr_plan* plan, int32_t bin, const void* ksp, void* image, void* stream);
+
+/* Batched coil/echo NUFFT on the internal layout (the PDHG hot path).
+ * forward: ksp[m, e, c] = F_b(images[e] * S_c)[m]            (images (E, Z, Y, X))
+ * adjoint: images[e] = sum_c conj(S_c) F_b^H(w[m] * ksp[m, e, c]),
+ *          w = plan dcf when use_dcf != 0, else 1. */
+tr_status tr_nufft_forward_bin(tr_plan* plan, int32_t bin, const void* images, void* ksp_internal,
+                               void* stream);
+tr_status tr_nufft_adjoint_bin(tr_plan* plan, int32_t bin, const void* ksp_internal, int32_t use_dcf,
+                               void* images, void* stream);
+
+/* PDHG (one device; all motion bins and echoes resident). */
+typedef struct {
+    int32_t algorithm;           /* TR_ALG_* */
+    int32_t l2_coupling;         /* --l2-coupling: prox over all echoes of the motion dual */
+    float sigma, tau;            /* dual / primal steps (reference: 1/6, tvme.py:968) */
+    float lam_m;                 /* motion TV (TVM lamda, TVME lamda_m, TVMW lambda1) */
+    float lam_e;                 /* TVME echo-spatial TV (lamda_e) */
+    float lam_w1;                /* TVMW db1 echo wavelet (lambda2) */
+    float lam_w2;                /* TVMW db6 spatial wavelet (lambda3) */
+    int32_t use_graph;           /* capture one iteration in a CUDA graph and replay it */
+} tr_pdhg_params;
+
+/* Device state, all (B, E, Z, Y, X) complex64 unless noted; unused fields NULL.
+ *   TVM / TVME: u = u_now, u_bar = the extrapolated iterate (the returned image).
+ *   TVMW:       u = primal_u_tmp, u_bar = primal_u (extrapolated, returned).
+ * q and y use the internal k-space layout, bins concatenated (bin offsets as in
+ * tr_plan_bin_offset * E * C).  g is scratch for the coil-combined adjoint;
+ * w2adj is TVMW scratch; p_w2 is (B*E, wavelet_coeffs). */
+typedef struct {
+    void* u;
+    void* u_bar;
+    void* p_m;
+    void* p_ex;
+    void* p_ey;
+    void* p_ez;
+    void* p_w1;
+    void* p_w2;
+    void* w2adj;
+    void* q;
+    const void* y;
+    void* g;
+} tr_pdhg_state;
+
+tr_status tr_plan_bin_offset(const tr_plan* plan, int32_t bin, int64_t* offset, int64_t* count);
+
+/* Runs up to max_iters iterations; stops after the first iteration whose
+ * tolerance is below tol (tvme.py:555, tvm.py:466, tvmw.py:772).
+ * tol_history (host, >= max_iters doubles, may be NULL) receives each
+ * iteration's tolerance; iters_done the number of iterations run. */
+tr_status tr_pdhg_run(tr_plan* plan, const tr_pdhg_state* state, const tr_pdhg_params* params,
+                      int32_t max_iters, double tol, double* tol_history, int32_t* iters_done,
+                      void* stream);
+
+/* Diagnostics in FP64: operator-norm estimate of A = F S (power iteration,
+ * n_iter steps) and the data residual 0.5*sum w |A u - y|^2. */
+tr_status tr_power_iteration(tr_plan* plan, int32_t n_iter, void* work_images, double* norm_out,
+                             void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TOPORECON_B200_H */

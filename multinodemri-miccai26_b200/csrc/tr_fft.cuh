@@ -1,0 +1,228 @@
+// Batched line FFTs in shared memory (mixed radix 2/3/4/5/7/8, Stockham auto-sort).
+//
+// A CTA transforms W independent columns of length L held as smem[L][W]
+// (column index fastest, so a warp touches whole 128-byte rows).  The stage
+// indexing is the Stockham formulation of Govindaraju et al. (SC'08):
+//   butterfly j < L/R reads   x[j + r L/R] * w_L^{(j mod Ns) r L/(Ns R)}
+//                 writes  y[(j / Ns) Ns R + (j mod Ns) + r Ns] = DFT_R(...)[r]
+// with Ns the product of the radices already applied.  The first stage reads
+// through a caller functor (global memory with pad / shift / fused scaling) and
+// the last stage writes through one (global memory with shift / crop, or a
+// shared-memory epilogue), so an L-point FFT with S stages makes 2(S-1) passes
+// over shared memory.  No normalisation is applied in either direction.
+#pragma once
+
+#include "tr_internal.cuh"
+
+namespace tr {
+
+// -i * z
+__device__ __forceinline__ float2 mul_mi(float2 z) { return make_float2(z.y, -z.x); }
+// +i * z
+__device__ __forceinline__ float2 mul_pi(float2 z) { return make_float2(-z.y, z.x); }
+
+template <int R>
+struct Dft;
+
+template <>
+struct Dft<2> {
+    __device__ __forceinline__ static void run(float2 (&v)[2], bool) {
+        float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    }
+};
+
+template <>
+struct Dft<4> {
+    __device__ __forceinline__ static void run(float2 (&v)[4], bool inv) {
+        float2 s0 = cadd(v[0], v[2]), d0 = csub(v[0], v[2]);
+        float2 s1 = cadd(v[1], v[3]), d1 = csub(v[1], v[3]);
+        float2 rd1 = inv ? mul_pi(d1) : mul_mi(d1);
+        v[0] = cadd(s0, s1);
+        v[2] = csub(s0, s1);
+        v[1] = cadd(d0, rd1);
+        v[3] = csub(d0, rd1);
+    }
+};
+
+template <>
+struct Dft<8> {
+    __device__ __forceinline__ static void run(float2 (&v)[8], bool inv) {
+        const float h = 0.70710678118654752f;
+        float2 a[4], b[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            a[r] = cadd(v[r], v[r + 4]);
+            b[r] = csub(v[r], v[r + 4]);
+        }
+        // b_r *= w_8^r  (forward w_8 = (1 - i)/sqrt2)
+        if (!inv) {
+            b[1] = make_float2(h * (b[1].x + b[1].y), h * (b[1].y - b[1].x));
+            b[2] = mul_mi(b[2]);
+            b[3] = make_float2(h * (b[3].y - b[3].x), -h * (b[3].x + b[3].y));
+        } else {
+            b[1] = make_float2(h * (b[1].x - b[1].y), h * (b[1].y + b[1].x));
+            b[2] = mul_pi(b[2]);
+            b[3] = make_float2(-h * (b[3].x + b[3].y), h * (b[3].x - b[3].y));
+        }
+        Dft<4>::run(a, inv);
+        Dft<4>::run(b, inv);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            v[2 * m] = a[m];
+            v[2 * m + 1] = b[m];
+        }
+    }
+};
+
+// Odd prime radices via conjugate-pair symmetry:
+//   X_m     = v0 + sum_r cos(2 pi r m / R) s_r  -/+ i sum_r sin(2 pi r m / R) d_r
+//   X_{R-m} = v0 + sum_r cos(2 pi r m / R) s_r  +/- i sum_r sin(2 pi r m / R) d_r
+// with s_r = v_r + v_{R-r}, d_r = v_r - v_{R-r} (upper sign: forward).
+template <int R>
+struct OddTables;
+template <>
+struct OddTables<3> {
+    __device__ __forceinline__ static float c(int k) { return -0.5f; }
+    __device__ __forceinline__ static float s(int k) { return 0.86602540378443865f; }
+};
+template <>
+struct OddTables<5> {
+    __device__ __forceinline__ static float c(int k) {
+        return k == 1 ? 0.30901699437494742f : -0.80901699437494742f;
+    }
+    __device__ __forceinline__ static float s(int k) {
+        return k == 1 ? 0.95105651629515357f : 0.58778525229247313f;
+    }
+};
+template <>
+struct OddTables<7> {
+    __device__ __forceinline__ static float c(int k) {
+        return k == 1 ? 0.62348980185873353f : (k == 2 ? -0.22252093395631440f : -0.90096886790241913f);
+    }
+    __device__ __forceinline__ static float s(int k) {
+        return k == 1 ? 0.78183148246802981f : (k == 2 ? 0.97492791218182361f : 0.43388373911755812f);
+    }
+};
+
+template <int R>
+struct DftOdd {
+    __device__ __forceinline__ static void run(float2 (&v)[R], bool inv) {
+        constexpr int H = (R - 1) / 2;
+        float2 s[H + 1], d[H + 1];
+#pragma unroll
+        for (int r = 1; r <= H; ++r) {
+            s[r] = cadd(v[r], v[R - r]);
+            d[r] = csub(v[r], v[R - r]);
+        }
+        float2 out[R];
+        float2 x0 = v[0];
+#pragma unroll
+        for (int r = 1; r <= H; ++r) x0 = cadd(x0, s[r]);
+        out[0] = x0;
+#pragma unroll
+        for (int m = 1; m <= H; ++m) {
+            float2 re = v[0], im = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int r = 1; r <= H; ++r) {
+                // angle index k = r*m mod R folded into [1, H] with a sign for the sine.
+                int k = (r * m) % R;
+                float sg = 1.f;
+                if (k > H) { k = R - k; sg = -1.f; }
+                float cv = OddTables<R>::c(k), sv = sg * OddTables<R>::s(k);
+                re = make_float2(re.x + cv * s[r].x, re.y + cv * s[r].y);
+                im = make_float2(im.x + sv * d[r].x, im.y + sv * d[r].y);
+            }
+            float2 t = inv ? mul_pi(im) : mul_mi(im);
+            out[m] = cadd(re, t);
+            out[R - m] = csub(re, t);
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[r] = out[r];
+    }
+};
+template <>
+struct Dft<3> : DftOdd<3> {};
+template <>
+struct Dft<5> : DftOdd<5> {};
+template <>
+struct Dft<7> : DftOdd<7> {};
+
+// One Stockham stage over every butterfly of every column.
+template <int R, class Src, class Dst>
+__device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, int L, int Ns, int W, bool inv,
+                                          Src src, Dst dst) {
+    const int nbf = L / R;
+    const int step = L / (Ns * R);
+    const int total = nbf * W;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int j = idx / W;
+        const int w = idx - j * W;
+        const int k = j % Ns;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            float2 x = src(j + r * nbf, w);
+            if (r > 0 && k > 0) {
+                float2 t = tw[k * r * step];
+                if (inv) t.y = -t.y;
+                x = cmul(x, t);
+            }
+            v[r] = x;
+        }
+        Dft<R>::run(v, inv);
+        const int d0 = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) dst(d0 + r * Ns, w, v[r]);
+    }
+}
+
+template <class Src, class Dst>
+__device__ __forceinline__ void fft_stage_dispatch(int R, const float2* tw, int L, int Ns, int W, bool inv,
+                                                   Src src, Dst dst) {
+    switch (R) {
+        case 2: fft_stage<2>(tw, L, Ns, W, inv, src, dst); break;
+        case 3: fft_stage<3>(tw, L, Ns, W, inv, src, dst); break;
+        case 4: fft_stage<4>(tw, L, Ns, W, inv, src, dst); break;
+        case 5: fft_stage<5>(tw, L, Ns, W, inv, src, dst); break;
+        case 7: fft_stage<7>(tw, L, Ns, W, inv, src, dst); break;
+        default: fft_stage<8>(tw, L, Ns, W, inv, src, dst); break;
+    }
+}
+
+// Full transform: load(m, w) -> input element m of column w; store(k, w, v)
+// receives output element k.  smA / smB are [L][W] scratch buffers.  The call
+// ends with a __syncthreads() only between stages; callers that read smem
+// written by `store` must synchronise themselves.
+template <class Load, class Store>
+__device__ __forceinline__ void fft_run(float2* smA, float2* smB, const float2* tw, const FftStages& S, int W,
+                                        bool inv, Load load, Store store) {
+    int Ns = 1;
+    for (int s = 0; s < S.nstages; ++s) {
+        const int R = S.radix[s];
+        const bool first = (s == 0), last = (s == S.nstages - 1);
+        float2* A = smA;
+        float2* Bf = smB;
+        auto smsrc = [A, W](int i, int w) { return A[i * W + w]; };
+        auto smdst = [Bf, W](int i, int w, float2 v) { Bf[i * W + w] = v; };
+        if (first && last) {
+            fft_stage_dispatch(R, tw, S.L, Ns, W, inv, load, store);
+        } else if (first) {
+            fft_stage_dispatch(R, tw, S.L, Ns, W, inv, load, smdst);
+        } else if (last) {
+            fft_stage_dispatch(R, tw, S.L, Ns, W, inv, smsrc, store);
+        } else {
+            fft_stage_dispatch(R, tw, S.L, Ns, W, inv, smsrc, smdst);
+        }
+        if (!last) {
+            __syncthreads();
+            float2* t = smA;
+            smA = smB;
+            smB = t;
+        }
+        Ns *= R;
+    }
+}
+
+}  // namespace tr

@@ -1,0 +1,150 @@
+// Internal definitions shared by the toporecon_b200 CUDA sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "toporecon_b200.h"
+
+namespace tr {
+
+// ------------------------------------------------------------------ errors
+void set_error(const std::string& msg);
+tr_status fail(tr_status code, const std::string& msg);
+tr_status cuda_fail(cudaError_t err, const char* what, const char* file, int line);
+
+#define TR_CUDA(expr)                                                   \
+    do {                                                                \
+        cudaError_t _e = (expr);                                        \
+        if (_e != cudaSuccess) return ::tr::cuda_fail(_e, #expr, __FILE__, __LINE__); \
+    } while (0)
+
+#define TR_CHECK_LAUNCH() TR_CUDA(cudaGetLastError())
+
+#define TR_TRY(expr)                                                    \
+    do {                                                                \
+        tr_status _s = (expr);                                          \
+        if (_s != TR_OK) return _s;                                     \
+    } while (0)
+
+// ------------------------------------------------------------------ complex helpers
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__host__ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__host__ __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
+
+// ------------------------------------------------------------------ FFT plan
+constexpr int kMaxStages = 12;
+constexpr int kMaxFftLen = 1024;
+
+struct FftAxis {
+    int n = 0;        // image length along the axis
+    int L = 0;        // oversampled (transform) length
+    int h = 0;        // centre shift L/2
+    int pad = 0;      // centred zero-pad offset L/2 - n/2
+    int nstages = 0;
+    int radix[kMaxStages] = {0};
+    float2* twiddle = nullptr;   // device [L]: exp(-2 pi i k / L)
+    float* apod = nullptr;       // device [n]: per-axis de-apodisation
+};
+
+// Per-launch description of the stage sequence, passed by value.
+struct FftStages {
+    int L;
+    int nstages;
+    int radix[kMaxStages];
+};
+
+inline FftStages stages_of(const FftAxis& a) {
+    FftStages s;
+    s.L = a.L;
+    s.nstages = a.nstages;
+    for (int i = 0; i < kMaxStages; ++i) s.radix[i] = a.radix[i];
+    return s;
+}
+
+// ------------------------------------------------------------------ plan
+struct Bin {
+    int64_t offset = 0;   // first sample of the bin in the concatenated arrays
+    int64_t count = 0;
+};
+
+struct PdhgGraph;        // defined in tr_pdhg.cu
+struct WaveletPlan;      // defined in tr_wavelet.cu
+
+}  // namespace tr
+
+struct tr_plan {
+    int device = 0;
+    int n[3] = {0, 0, 0};     // Z, Y, X
+    int os[3] = {0, 0, 0};
+    int C = 1, E = 1, B = 1;
+    float beta = 0.f;
+    int width = 4;
+    float fwd_scale = 1.f;    // 1 / (sqrt(N) * w^3)
+    float adj_scale = 1.f;    // 1 / (sqrt(N) * w^3)
+    tr::FftAxis ax[3];
+    std::vector<tr::Bin> bins;
+    int64_t total = 0;
+    // device-resident trajectory (tile-sorted per bin)
+    float4* ks = nullptr;        // (kz, ky, kx, dcf) in oversampled-grid units, sorted
+    int32_t* perm = nullptr;     // sorted position -> acquisition index within the bin
+    int32_t* tile_start = nullptr;  // per bin [ntiles + 1] (relative to the bin offset)
+    int32_t* tile_order = nullptr;  // per bin [ntiles]: heaviest tiles first
+    int ntile[3] = {0, 0, 0};
+    int64_t ntiles = 0;
+    bool has_dcf = false;
+    // coil maps (Z, Y, X, C) interleaved
+    float2* maps = nullptr;
+    // NUFFT workspace
+    float2* bufA = nullptr;      // >= OSZ*OSY*OSX*ncol (grid / x-pass output)
+    float2* bufB = nullptr;      // >= Z*OSY*OSX*ncol  (y-pass output / z-pass adjoint output)
+    size_t buf_cols = 0;         // ncol the buffers are sized for
+    // single-image drop-in scratch
+    float2* one_in = nullptr;
+    float2* one_out = nullptr;
+    size_t one_elems = 0;
+    // reductions
+    double* partials = nullptr;
+    int npartials = 0;
+    double* tol_dev = nullptr;   // [4]
+    double* tol_host = nullptr;  // pinned [4]
+    // launch shapes
+    int line_width = 16;
+    // TVMW
+    tr::WaveletPlan* wav = nullptr;
+    // CUDA graph of one PDHG iteration
+    tr::PdhgGraph* graph = nullptr;
+    int64_t workspace_bytes = 0;
+};
+
+namespace tr {
+
+tr_status ensure_nufft_buffers(tr_plan* p, size_t ncol);
+tr_status nufft_forward_cols(tr_plan* p, int bin, const float2* images, int64_t img_stride, int n_img,
+                             const float2* maps, int C, int mode, float sigma, const float2* y,
+                             float2* out, cudaStream_t st);
+tr_status nufft_adjoint_cols(tr_plan* p, int bin, const float2* ksp, int n_img, const float2* maps, int C,
+                             bool use_dcf, float2* images, int64_t img_stride, cudaStream_t st);
+tr_status wavelet_prepare(tr_plan* p);
+tr_status wavelet_dual(tr_plan* p, const float2* u_bar, float2* p_w2, float sigma, float lam, cudaStream_t st);
+tr_status wavelet_adjoint(tr_plan* p, const float2* p_w2, float2* out, cudaStream_t st);
+void wavelet_destroy(tr_plan* p);
+void wavelet_info(const tr_plan* p, int32_t* levels, int64_t* coeffs);
+void pdhg_destroy(tr_plan* p);
+
+// forward interpolation output modes
+constexpr int kInterpStore = 0;     // out = A x
+constexpr int kInterpDualProx = 1;  // out = (out + sigma (A x - y)) / (1 + sigma)
+
+}  // namespace tr

@@ -1,0 +1,1117 @@
+// Kaiser-Bessel NUFFT for sm_100a: plan (tile sort), fused FFT passes,
+// interpolation and deterministic tile-gather gridding, and their C ABI.
+//
+// Numerical definition (the reference's SigPy 0.1.27 defaults, called at
+// src/toporecon/nufft_backend.py:104-107 and :112-116):
+//   forward  y = I_KB( FFTc( pad( apod . x ) ) ) / (sqrt(N) w^3)
+//   adjoint  x = apod . crop( IFFTc( G_KB(y) ) ) / (sqrt(N) w^3)
+// with oversampling 1.25, width w = 4, beta = pi sqrt((w/os (os - 0.5))^2 - 0.8),
+// taps ceil(k - 2) .. floor(k + 2) per axis and periodic wrap.
+//
+// Data layout (device):
+//   images           (n_img, Z, Y, X)                  complex64
+//   coil maps        (Z, Y, X, C)                      complex64, plan-owned copy
+//   x-pass buffer    (Z, Y, OSX, ncol)                 ncol = n_img * C columns
+//   y-pass buffer    (Z, OSY, OSX, ncol)
+//   grid             (OSZ, OSY, OSX, ncol)
+//   k-space          (M_b, ncol) per bin, tile-sorted samples
+// The trajectory of each bin is sorted by 4x4x4 grid tile (stable counting
+// sort on the host, so the gather order and hence every sum is deterministic).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "tr_fft.cuh"
+#include "tr_internal.cuh"
+
+namespace tr {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+tr_status fail(tr_status code, const std::string& msg) {
+    set_error(msg);
+    return code;
+}
+
+tr_status cuda_fail(cudaError_t err, const char* what, const char* file, int line) {
+    char buf[512];
+    snprintf(buf, sizeof(buf), "CUDA error %d (%s) in %s at %s:%d", (int)err, cudaGetErrorString(err), what,
+             file, line);
+    set_error(buf);
+    return err == cudaErrorMemoryAllocation ? TR_ERR_OOM : TR_ERR_CUDA;
+}
+
+// ------------------------------------------------------------------ KB window
+// Modified Bessel I0 by the Abramowitz & Stegun 9.8.1 / 9.8.2 approximations
+// (the same published formulas SigPy evaluates), then the unnormalised window.
+__host__ __device__ __forceinline__ float bessel_i0_as(float x) {
+    if (x < 3.75f) {
+        float t = x * (1.0f / 3.75f);
+        float t2 = t * t;
+        return 1.0f + t2 * (3.5156229f + t2 * (3.0899424f + t2 * (1.2067492f +
+               t2 * (0.2659732f + t2 * (0.0360768f + t2 * 0.0045813f)))));
+    }
+    float u = 3.75f / x;
+    float poly = 0.39894228f + u * (0.01328592f + u * (0.00225319f + u * (-0.00157565f + u * (0.00916281f +
+                 u * (-0.02057706f + u * (0.02635537f + u * (-0.01647633f + u * 0.00392377f)))))));
+    return expf(x) * rsqrtf(x) * poly;
+}
+
+__device__ __forceinline__ float kb_weight(float d, float beta) {
+    // d = (tap - k) / (w / 2); zero outside |d| <= 1
+    if (fabsf(d) > 1.0f) return 0.0f;
+    return bessel_i0_as(beta * sqrtf(fmaxf(1.0f - d * d, 0.0f)));
+}
+
+__device__ __forceinline__ int pmod(int a, int n) {
+    int r = a % n;
+    return r < 0 ? r + n : r;
+}
+
+// First tap and the five candidate weights of one axis (w = 4).
+__device__ __forceinline__ int axis_taps(float k, float beta, float (&w)[5]) {
+    // ceil(k - w/2) evaluated in double like the reference's tap bounds
+    const int b0 = (int)ceil((double)k - 2.0);
+#pragma unroll
+    for (int t = 0; t < 5; ++t) w[t] = kb_weight(((float)(b0 + t) - k) * 0.5f, beta);
+    return b0;
+}
+
+// ------------------------------------------------------------------ forward x pass
+// One CTA: `rows` consecutive (z, y) image rows x `cc` coils of one image.
+// Fuses: image * coil map * separable apodisation * scale, centred zero-pad,
+// x FFT, centred shift; output into the (Z, Y, OSX, ncol) buffer.
+struct FwdXArgs {
+    const float2* img;      // (n_img, Z, Y, X)
+    int64_t img_stride;
+    const float2* maps;     // (Z, Y, X, C) or null
+    int C;                  // coils per image (1 when maps == null)
+    int n_img;
+    int Z, Y, X, OSX, h, pad;
+    int rows, cc;           // rows per CTA, coils per CTA
+    const float* apz;
+    const float* apy;
+    const float* apx;
+    float scale;
+    const float2* tw;
+    FftStages S;
+    float2* out;            // (Z, Y, OSX, ncol)
+    int ncol;
+};
+
+__global__ void __launch_bounds__(256) k_fwd_x(FwdXArgs a) {
+    extern __shared__ float2 sm[];
+    const int W = a.rows * a.cc;
+    float2* smA = sm;
+    float2* smB = sm + a.S.L * W;
+    float2* tws = sm + 2 * a.S.L * W;
+    for (int i = threadIdx.x; i < a.S.L; i += blockDim.x) tws[i] = a.tw[i];
+    __syncthreads();
+    const int row0 = blockIdx.x * a.rows;
+    const int img = blockIdx.y;
+    const int c0 = blockIdx.z * a.cc;
+    const int nrows = a.Z * a.Y;
+    const float2* __restrict__ src = a.img + (int64_t)img * a.img_stride;
+    auto load = [&](int m, int w) -> float2 {
+        const int rl = w / a.cc, cl = w - rl * a.cc;
+        const int row = row0 + rl;
+        const int c = c0 + cl;
+        int j = m + a.h;
+        if (j >= a.S.L) j -= a.S.L;
+        const int x = j - a.pad;
+        if (x < 0 || x >= a.X || row >= nrows || c >= a.C) return make_float2(0.f, 0.f);
+        const int z = row / a.Y, y = row - z * a.Y;
+        float2 v = src[(int64_t)row * a.X + x];
+        if (a.maps) v = cmul(v, a.maps[((int64_t)row * a.X + x) * a.C + c]);
+        const float s = a.apz[z] * a.apy[y] * a.apx[x] * a.scale;
+        return cscale(v, s);
+    };
+    auto store = [&](int k, int w, float2 v) {
+        const int rl = w / a.cc, cl = w - rl * a.cc;
+        const int row = row0 + rl;
+        const int c = c0 + cl;
+        if (row >= nrows || c >= a.C) return;
+        int g = k + a.h;
+        if (g >= a.S.L) g -= a.S.L;
+        a.out[((int64_t)row * a.OSX + g) * a.ncol + (int64_t)img * a.C + c] = v;
+    };
+    fft_run(smA, smB, tws, a.S, W, false, load, store);
+}
+
+// ------------------------------------------------------------------ generic line pass
+// Data viewed as [outer][rows][inner]; transforms along rows for W consecutive
+// inner elements per CTA.  Input rows present: Lin (pad offset p_in inside the
+// length-L line); output rows kept: Lout (crop offset p_out).
+struct LineArgs {
+    const float2* in;
+    float2* out;
+    int64_t inner;
+    int Lin, Lout, p_in, p_out, h;
+    int W;
+    bool inv;
+    const float2* tw;
+    FftStages S;
+};
+
+__global__ void __launch_bounds__(256) k_line(LineArgs a) {
+    extern __shared__ float2 sm[];
+    const int W = a.W;
+    float2* smA = sm;
+    float2* smB = sm + a.S.L * W;
+    float2* tws = sm + 2 * a.S.L * W;
+    for (int i = threadIdx.x; i < a.S.L; i += blockDim.x) tws[i] = a.tw[i];
+    __syncthreads();
+    const int64_t q0 = (int64_t)blockIdx.x * W;
+    const int64_t outer = blockIdx.y;
+    const float2* __restrict__ in = a.in + outer * a.Lin * a.inner;
+    float2* __restrict__ out = a.out + outer * a.Lout * a.inner;
+    const int L = a.S.L;
+    auto load = [&](int m, int w) -> float2 {
+        const int64_t q = q0 + w;
+        int j = m + a.h;
+        if (j >= L) j -= L;
+        const int i = j - a.p_in;
+        if (q >= a.inner || i < 0 || i >= a.Lin) return make_float2(0.f, 0.f);
+        return in[(int64_t)i * a.inner + q];
+    };
+    auto store = [&](int k, int w, float2 v) {
+        const int64_t q = q0 + w;
+        int o = k + a.h - a.p_out;
+        o = o % L;
+        if (o < 0) o += L;
+        if (q >= a.inner || o >= a.Lout) return;
+        out[(int64_t)o * a.inner + q] = v;
+    };
+    fft_run(smA, smB, tws, a.S, W, a.inv, load, store);
+}
+
+// ------------------------------------------------------------------ adjoint x pass
+// One CTA: `rows` rows x all C coils of one image (coils processed in chunks
+// of `cc`).  Fuses: x IFFT, centred shift and crop, apodisation, scale,
+// conj(coil map) and the coil sum; writes (or adds into) the image row.
+struct AdjXArgs {
+    const float2* in;       // (Z, Y, OSX, ncol)
+    int ncol;
+    const float2* maps;     // (Z, Y, X, C) or null
+    int C, cc, rows;
+    int Z, Y, X, OSX, h, pad;
+    const float* apz;
+    const float* apy;
+    const float* apx;
+    float scale;
+    const float2* tw;
+    FftStages S;
+    float2* img;            // (n_img, Z, Y, X)
+    int64_t img_stride;
+    int accumulate;
+};
+
+__global__ void __launch_bounds__(256) k_adj_x(AdjXArgs a) {
+    extern __shared__ float2 sm[];
+    const int W = a.rows * a.cc;
+    const int L = a.S.L;
+    float2* buf0 = sm;
+    float2* buf1 = sm + L * W;
+    float2* tws = sm + 2 * L * W;
+    float2* acc = tws + L;                  // [rows][X]
+    for (int i = threadIdx.x; i < L; i += blockDim.x) tws[i] = a.tw[i];
+    for (int i = threadIdx.x; i < a.rows * a.X; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
+    __syncthreads();
+    const int row0 = blockIdx.x * a.rows;
+    const int img = blockIdx.y;
+    const int nrows = a.Z * a.Y;
+    // buffer free during the last stage (the other one is its source)
+    float2* ep = (a.S.nstages == 1) ? buf1 : (((a.S.nstages - 1) % 2 == 0) ? buf1 : buf0);
+    for (int c0 = 0; c0 < a.C; c0 += a.cc) {
+        auto load = [&](int m, int w) -> float2 {
+            const int rl = w / a.cc, cl = w - rl * a.cc;
+            const int row = row0 + rl, c = c0 + cl;
+            if (row >= nrows || c >= a.C) return make_float2(0.f, 0.f);
+            int j = m + a.h;
+            if (j >= L) j -= L;
+            return a.in[((int64_t)row * a.OSX + j) * a.ncol + (int64_t)img * a.C + c];
+        };
+        auto store = [&](int k, int w, float2 v) {
+            int o = k + a.h - a.pad;
+            o %= L;
+            if (o < 0) o += L;
+            if (o < a.X) ep[o * W + w] = v;
+        };
+        fft_run(buf0, buf1, tws, a.S, W, true, load, store);
+        __syncthreads();
+        for (int i = threadIdx.x; i < a.rows * a.X; i += blockDim.x) {
+            const int rl = i / a.X, x = i - rl * a.X;
+            const int row = row0 + rl;
+            if (row >= nrows) continue;
+            float2 s = acc[i];
+            for (int cl = 0; cl < a.cc && c0 + cl < a.C; ++cl) {
+                float2 v = ep[x * W + rl * a.cc + cl];
+                if (a.maps) v = cmulc(v, a.maps[((int64_t)row * a.X + x) * a.C + c0 + cl]);
+                s = cadd(s, v);
+            }
+            acc[i] = s;
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < a.rows * a.X; i += blockDim.x) {
+        const int rl = i / a.X, x = i - rl * a.X;
+        const int row = row0 + rl;
+        if (row >= nrows) continue;
+        const int z = row / a.Y, y = row - z * a.Y;
+        const float s = a.apz[z] * a.apy[y] * a.apx[x] * a.scale;
+        float2 v = cscale(acc[i], s);
+        float2* dst = a.img + (int64_t)img * a.img_stride + (int64_t)row * a.X + x;
+        if (a.accumulate) v = cadd(*dst, v);
+        *dst = v;
+    }
+}
+
+// ------------------------------------------------------------------ interpolation
+// G lanes cooperate on one sample (lane = column group); taps read ncol
+// contiguous complex values per grid point (coalesced across lanes).
+template <int CPL>
+__global__ void __launch_bounds__(256) k_interp(const float2* __restrict__ grid, const float4* __restrict__ ks,
+                                                int64_t M, int ncol, int G, int os0, int os1, int os2, float beta,
+                                                int mode, float sigma, const float2* __restrict__ y,
+                                                float2* __restrict__ out) {
+    const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t s = gt / G;
+    const int lane = (int)(gt - s * G);
+    if (s >= M) return;
+    const float4 kk = ks[s];
+    float wz[5], wy[5], wx[5];
+    const int bz = axis_taps(kk.x, beta, wz);
+    const int by = axis_taps(kk.y, beta, wy);
+    const int bx = axis_taps(kk.z, beta, wx);
+    int iy[5], ix[5];
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+        iy[t] = pmod(by + t, os1);
+        ix[t] = pmod(bx + t, os2);
+    }
+    float2 acc[CPL];
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) acc[j] = make_float2(0.f, 0.f);
+#pragma unroll 1
+    for (int tz = 0; tz < 5; ++tz) {
+        if (wz[tz] == 0.f) continue;
+        const int64_t zoff = (int64_t)pmod(bz + tz, os0) * os1;
+#pragma unroll 1
+        for (int ty = 0; ty < 5; ++ty) {
+            if (wy[ty] == 0.f) continue;
+            const float wzy = wz[tz] * wy[ty];
+            const int64_t yoff = (zoff + iy[ty]) * os2;
+#pragma unroll
+            for (int tx = 0; tx < 5; ++tx) {
+                if (wx[tx] == 0.f) continue;
+                const float w = wzy * wx[tx];
+                const float2* gp = grid + (yoff + ix[tx]) * ncol;
+#pragma unroll
+                for (int j = 0; j < CPL; ++j) {
+                    const int col = lane + j * G;
+                    if (col < ncol) {
+                        const float2 g = gp[col];
+                        acc[j].x += w * g.x;
+                        acc[j].y += w * g.y;
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < CPL; ++j) {
+        const int col = lane + j * G;
+        if (col >= ncol) continue;
+        const int64_t o = s * ncol + col;
+        if (mode == kInterpDualProx) {
+            const float2 r = csub(acc[j], y[o]);
+            const float2 q = out[o];
+            const float inv = 1.0f / (1.0f + sigma);
+            out[o] = make_float2((q.x + sigma * r.x) * inv, (q.y + sigma * r.y) * inv);
+        } else {
+            out[o] = acc[j];
+        }
+    }
+}
+
+// ------------------------------------------------------------------ gridding (tile gather)
+// One CTA owns a 4x4x4 tile of the oversampled grid and all ncc columns of the
+// chunk.  Candidate samples come from the 27 neighbouring tiles of the sorted
+// trajectory; those whose support meets the tile are compacted (in candidate
+// order) with their per-axis weights, their values staged in shared memory,
+// and every (point, column) accumulator sums over them in that fixed order.
+// No atomics: the result is bitwise reproducible.
+constexpr int kTile = 4;
+constexpr int kTilePts = kTile * kTile * kTile;
+
+struct SpreadArgs {
+    const float4* ks;          // bin base
+    const int32_t* tile_start; // bin base [ntiles + 1]
+    const int32_t* tile_order; // bin base [ntiles] or null
+    const float2* vals;        // (M_b, ncol) bin base
+    int ncol, col0, ncc;
+    int use_dcf;
+    float2* grid;              // (OSZ, OSY, OSX, ncol)
+    int os0, os1, os2;
+    int nt0, nt1, nt2;
+    float beta;
+    int K;                     // candidates per chunk
+};
+
+template <int CPT>
+__global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ int run_start[27];
+    __shared__ int run_pref[28];
+    __shared__ int warp_cnt[8];
+    __shared__ int warp_off[9];
+    const int K = a.K;
+    int* c_rel = reinterpret_cast<int*>(smraw);                  // [K][3]
+    float* c_w = reinterpret_cast<float*>(c_rel + 3 * K);        // [K][15]
+    int* c_s = reinterpret_cast<int*>(c_w + 15 * K);             // [K]
+    float* c_d = reinterpret_cast<float*>(c_s + K);              // [K]
+    float2* dq = reinterpret_cast<float2*>(c_d + K);             // [max(K, 64)][ncc] (80 K bytes in: 8-aligned)
+
+    const int tile = a.tile_order ? a.tile_order[blockIdx.x] : (int)blockIdx.x;
+    const int tz = tile / (a.nt1 * a.nt2);
+    const int trem = tile - tz * a.nt1 * a.nt2;
+    const int ty = trem / a.nt2;
+    const int tx = trem - ty * a.nt2;
+    const int t0z = tz * kTile, t0y = ty * kTile, t0x = tx * kTile;
+    const int Tz = min(kTile, a.os0 - t0z), Ty = min(kTile, a.os1 - t0y), Tx = min(kTile, a.os2 - t0x);
+
+    const int tid = threadIdx.x;
+    if (tid < 27) {
+        const int dz = tid / 9 - 1, dy = (tid / 3) % 3 - 1, dx = tid % 3 - 1;
+        const int nz = pmod(tz + dz, a.nt0), ny = pmod(ty + dy, a.nt1), nx = pmod(tx + dx, a.nt2);
+        const int id = (nz * a.nt1 + ny) * a.nt2 + nx;
+        run_start[tid] = a.tile_start[id];
+        run_pref[tid + 1] = a.tile_start[id + 1] - a.tile_start[id];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        run_pref[0] = 0;
+        for (int r = 0; r < 27; ++r) run_pref[r + 1] += run_pref[r];
+    }
+    __syncthreads();
+    const int total = run_pref[27];
+
+    const int p = tid & 63;
+    const int pz = p >> 4, py = (p >> 2) & 3, px = p & 3;
+    const int cs = tid >> 6;
+    float2 acc[CPT];
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) acc[j] = make_float2(0.f, 0.f);
+
+    const int lane = tid & 31, warp = tid >> 5;
+    for (int base = 0; base < total; base += K) {
+        // ---- phase 1: candidate test and deterministic compaction
+        int flag = 0, rel[3] = {0, 0, 0}, sidx = 0;
+        float4 kk = make_float4(0.f, 0.f, 0.f, 0.f);
+        const int ci = base + tid;
+        if (tid < K && ci < total) {
+            int r = 0;
+            while (run_pref[r + 1] <= ci) ++r;
+            sidx = run_start[r] + (ci - run_pref[r]);
+            kk = a.ks[sidx];
+            const float kc[3] = {kk.x, kk.y, kk.z};
+            const int t0[3] = {t0z, t0y, t0x};
+            const int Tn[3] = {Tz, Ty, Tx};
+            const int osn[3] = {a.os0, a.os1, a.os2};
+            flag = 1;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const int b0 = (int)ceil((double)kc[d] - 2.0);
+                int rr = pmod(t0[d] - b0, osn[d]);
+                if (rr > 4) rr -= osn[d];
+                rel[d] = rr;
+                if (rr > 4 || rr + Tn[d] - 1 < 0) flag = 0;
+            }
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, flag);
+        if (lane == 0) warp_cnt[warp] = __popc(bal);
+        __syncthreads();
+        if (tid == 0) {
+            warp_off[0] = 0;
+            for (int w = 0; w < 8; ++w) warp_off[w + 1] = warp_off[w] + warp_cnt[w];
+        }
+        __syncthreads();
+        const int nc = warp_off[8];
+        if (flag) {
+            const int pos = warp_off[warp] + __popc(bal & ((1u << lane) - 1u));
+            c_rel[3 * pos + 0] = rel[0];
+            c_rel[3 * pos + 1] = rel[1];
+            c_rel[3 * pos + 2] = rel[2];
+            float w5[5];
+            axis_taps(kk.x, a.beta, w5);
+#pragma unroll
+            for (int t = 0; t < 5; ++t) c_w[15 * pos + t] = w5[t];
+            axis_taps(kk.y, a.beta, w5);
+#pragma unroll
+            for (int t = 0; t < 5; ++t) c_w[15 * pos + 5 + t] = w5[t];
+            axis_taps(kk.z, a.beta, w5);
+#pragma unroll
+            for (int t = 0; t < 5; ++t) c_w[15 * pos + 10 + t] = w5[t];
+            c_s[pos] = sidx;
+            c_d[pos] = a.use_dcf ? kk.w : 1.0f;
+        }
+        __syncthreads();
+        // ---- phase 2: stage weighted values
+        for (int i = tid; i < nc * a.ncc; i += blockDim.x) {
+            const int cand = i / a.ncc, col = i - cand * a.ncc;
+            float2 v = a.vals[(int64_t)c_s[cand] * a.ncol + a.col0 + col];
+            dq[i] = cscale(v, c_d[cand]);
+        }
+        __syncthreads();
+        // ---- phase 3: gather-accumulate in candidate order
+        for (int cc = 0; cc < nc; ++cc) {
+            const int az = c_rel[3 * cc + 0] + pz;
+            const int ay = c_rel[3 * cc + 1] + py;
+            const int ax = c_rel[3 * cc + 2] + px;
+            if ((unsigned)az > 4u || (unsigned)ay > 4u || (unsigned)ax > 4u) continue;
+            const float w = c_w[15 * cc + az] * c_w[15 * cc + 5 + ay] * c_w[15 * cc + 10 + ax];
+            if (w == 0.f) continue;
+            const float2* row = dq + cc * a.ncc;
+#pragma unroll
+            for (int j = 0; j < CPT; ++j) {
+                const int col = cs + 4 * j;
+                if (col < a.ncc) {
+                    const float2 v = row[col];
+                    acc[j].x += w * v.x;
+                    acc[j].y += w * v.y;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // ---- stage the tile in shared memory and write it out coalesced
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) {
+        const int col = cs + 4 * j;
+        if (col < a.ncc) dq[p * a.ncc + col] = acc[j];
+    }
+    __syncthreads();
+    for (int i = tid; i < kTilePts * a.ncc; i += blockDim.x) {
+        const int pp = i / a.ncc, col = i - pp * a.ncc;
+        const int qz = pp >> 4, qy = (pp >> 2) & 3, qx = pp & 3;
+        if (qz >= Tz || qy >= Ty || qx >= Tx) continue;
+        const int64_t g = ((int64_t)(t0z + qz) * a.os1 + (t0y + qy)) * a.os2 + (t0x + qx);
+        a.grid[g * a.ncol + a.col0 + col] = dq[i];
+    }
+}
+
+// ------------------------------------------------------------------ sample order conversion
+__global__ void k_sort_ksp(const float2* __restrict__ ext, float2* __restrict__ internal, const int32_t* __restrict__ perm,
+                           int64_t M, int ncol) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M * ncol) return;
+    const int64_t s = i / ncol;
+    const int col = (int)(i - s * ncol);
+    internal[i] = ext[(int64_t)col * M + perm[s]];
+}
+
+__global__ void k_unsort_ksp(const float2* __restrict__ internal, float2* __restrict__ ext, const int32_t* __restrict__ perm,
+                             int64_t M, int ncol) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M * ncol) return;
+    const int64_t s = i / ncol;
+    const int col = (int)(i - s * ncol);
+    ext[(int64_t)col * M + perm[s]] = internal[i];
+}
+
+// (Z, Y, X, C) <- (C, Z, Y, X)
+__global__ void k_interleave_maps(const float2* __restrict__ src, float2* __restrict__ dst, int64_t N, int C) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N * C) return;
+    const int64_t v = i / C;
+    const int c = (int)(i - v * C);
+    dst[i] = src[(int64_t)c * N + v];
+}
+
+// ------------------------------------------------------------------ host helpers
+static bool factor_radices(int L, int* radix, int* nstages) {
+    int n = L, s = 0;
+    for (int r : {7, 5, 3}) {
+        while (n % r == 0) {
+            if (s >= kMaxStages) return false;
+            radix[s++] = r;
+            n /= r;
+        }
+    }
+    while (n % 8 == 0) {
+        if (s >= kMaxStages) return false;
+        radix[s++] = 8;
+        n /= 8;
+    }
+    while (n % 4 == 0) {
+        if (s >= kMaxStages) return false;
+        radix[s++] = 4;
+        n /= 4;
+    }
+    while (n % 2 == 0) {
+        if (s >= kMaxStages) return false;
+        radix[s++] = 2;
+        n /= 2;
+    }
+    *nstages = s;
+    return n == 1;
+}
+
+static size_t fft_smem_bytes(int L, int W) { return (size_t)(2 * L * W + L) * sizeof(float2); }
+
+static tr_status set_smem_limit(const void* fn, size_t bytes) {
+    if (bytes > 48 * 1024) TR_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    return TR_OK;
+}
+
+tr_status ensure_nufft_buffers(tr_plan* p, size_t ncol) {
+    if (p->bufA && p->buf_cols >= ncol) return TR_OK;
+    if (p->bufA) cudaFree(p->bufA);
+    if (p->bufB) cudaFree(p->bufB);
+    p->bufA = p->bufB = nullptr;
+    const size_t gA = (size_t)p->os[0] * p->os[1] * p->os[2] * ncol;
+    const size_t gB = (size_t)p->n[0] * p->os[1] * p->os[2] * ncol;
+    TR_CUDA(cudaMalloc(&p->bufA, gA * sizeof(float2)));
+    TR_CUDA(cudaMalloc(&p->bufB, gB * sizeof(float2)));
+    p->workspace_bytes += (int64_t)((gA + gB) * sizeof(float2));
+    p->buf_cols = ncol;
+    return TR_OK;
+}
+
+static tr_status launch_line(tr_plan* p, int axis, const float2* in, float2* out, int64_t outer, int64_t inner,
+                             int Lin, int Lout, int p_in, int p_out, bool inv, cudaStream_t st) {
+    const FftAxis& A = p->ax[axis];
+    LineArgs la;
+    la.in = in;
+    la.out = out;
+    la.inner = inner;
+    la.Lin = Lin;
+    la.Lout = Lout;
+    la.p_in = p_in;
+    la.p_out = p_out;
+    la.h = A.h;
+    la.W = p->line_width;
+    la.inv = inv;
+    la.tw = A.twiddle;
+    la.S = stages_of(A);
+    const size_t smem = fft_smem_bytes(A.L, la.W);
+    TR_TRY(set_smem_limit((const void*)k_line, smem));
+    dim3 grid((unsigned)((inner + la.W - 1) / la.W), (unsigned)outer);
+    k_line<<<grid, 256, smem, st>>>(la);
+    TR_CHECK_LAUNCH();
+    return TR_OK;
+}
+
+static int coils_per_cta(int C) { return C <= 32 ? C : 32; }
+
+tr_status nufft_forward_cols(tr_plan* p, int bin, const float2* images, int64_t img_stride, int n_img,
+                             const float2* maps, int C, int mode, float sigma, const float2* y, float2* out,
+                             cudaStream_t st) {
+    const int ncol = n_img * C;
+    TR_TRY(ensure_nufft_buffers(p, (size_t)ncol));
+    const int Z = p->n[0], Y = p->n[1], X = p->n[2];
+    const int OSZ = p->os[0], OSY = p->os[1], OSX = p->os[2];
+    // x pass
+    FwdXArgs fa;
+    fa.img = images;
+    fa.img_stride = img_stride;
+    fa.maps = maps;
+    fa.C = C;
+    fa.n_img = n_img;
+    fa.Z = Z;
+    fa.Y = Y;
+    fa.X = X;
+    fa.OSX = OSX;
+    fa.h = p->ax[2].h;
+    fa.pad = p->ax[2].pad;
+    fa.cc = coils_per_cta(C);
+    fa.rows = std::max(1, 16 / fa.cc);
+    fa.apz = p->ax[0].apod;
+    fa.apy = p->ax[1].apod;
+    fa.apx = p->ax[2].apod;
+    fa.scale = p->fwd_scale;
+    fa.tw = p->ax[2].twiddle;
+    fa.S = stages_of(p->ax[2]);
+    fa.out = p->bufA;
+    fa.ncol = ncol;
+    {
+        const int W = fa.rows * fa.cc;
+        const size_t smem = fft_smem_bytes(OSX, W);
+        TR_TRY(set_smem_limit((const void*)k_fwd_x, smem));
+        dim3 grid((unsigned)((Z * Y + fa.rows - 1) / fa.rows), (unsigned)n_img, (unsigned)((C + fa.cc - 1) / fa.cc));
+        k_fwd_x<<<grid, 256, smem, st>>>(fa);
+        TR_CHECK_LAUNCH();
+    }
+    // y pass: [Z][Y -> OSY][OSX * ncol]
+    TR_TRY(launch_line(p, 1, p->bufA, p->bufB, Z, (int64_t)OSX * ncol, Y, OSY, p->ax[1].pad, 0, false, st));
+    // z pass: [1][Z -> OSZ][OSY * OSX * ncol]
+    TR_TRY(launch_line(p, 0, p->bufB, p->bufA, 1, (int64_t)OSY * OSX * ncol, Z, OSZ, p->ax[0].pad, 0, false, st));
+    // interpolation
+    const Bin& b = p->bins[bin];
+    if (b.count == 0) return TR_OK;
+    int G = 1;
+    while (G < ncol && G < 32) G <<= 1;
+    const int cpl = (ncol + G - 1) / G;
+    const int64_t threads = b.count * G;
+    const unsigned blocks = (unsigned)((threads + 255) / 256);
+    const float4* ks = p->ks + b.offset;
+#define TR_INTERP(CPLV)                                                                                      \
+    k_interp<CPLV><<<blocks, 256, 0, st>>>(p->bufA, ks, b.count, ncol, G, OSZ, OSY, OSX, p->beta, mode, sigma, y, \
+                                           out)
+    if (cpl <= 1) TR_INTERP(1);
+    else if (cpl <= 2) TR_INTERP(2);
+    else if (cpl <= 3) TR_INTERP(3);
+    else if (cpl <= 4) TR_INTERP(4);
+    else if (cpl <= 8) TR_INTERP(8);
+    else return fail(TR_ERR_UNSUPPORTED, "more than 256 k-space columns per bin are not supported");
+#undef TR_INTERP
+    TR_CHECK_LAUNCH();
+    return TR_OK;
+}
+
+template <int CPT>
+static tr_status launch_spread_t(const SpreadArgs& sa, unsigned ntiles, cudaStream_t st) {
+    const size_t cand_bytes = (size_t)sa.K * (3 * 4 + 15 * 4 + 4 + 4) + 8;
+    const size_t dq_bytes = (size_t)std::max(sa.K, kTilePts) * sa.ncc * sizeof(float2);
+    const size_t smem = cand_bytes + dq_bytes;
+    TR_TRY(set_smem_limit((const void*)k_spread<CPT>, smem));
+    k_spread<CPT><<<ntiles, 256, smem, st>>>(sa);
+    TR_CHECK_LAUNCH();
+    return TR_OK;
+}
+
+tr_status nufft_adjoint_cols(tr_plan* p, int bin, const float2* ksp, int n_img, const float2* maps, int C,
+                             bool use_dcf, float2* images, int64_t img_stride, cudaStream_t st) {
+    const int ncol = n_img * C;
+    TR_TRY(ensure_nufft_buffers(p, (size_t)ncol));
+    const int Z = p->n[0], Y = p->n[1], X = p->n[2];
+    const int OSZ = p->os[0], OSY = p->os[1], OSX = p->os[2];
+    const Bin& b = p->bins[bin];
+    // gridding, in column chunks of at most 128
+    for (int col0 = 0; col0 < ncol; col0 += 128) {
+        SpreadArgs sa;
+        sa.ks = p->ks + b.offset;
+        sa.tile_start = p->tile_start + (int64_t)bin * (p->ntiles + 1);
+        sa.tile_order = p->tile_order + (int64_t)bin * p->ntiles;
+        sa.vals = ksp;
+        sa.ncol = ncol;
+        sa.col0 = col0;
+        sa.ncc = std::min(128, ncol - col0);
+        sa.use_dcf = (use_dcf && p->has_dcf) ? 1 : 0;
+        sa.grid = p->bufA;
+        sa.os0 = OSZ;
+        sa.os1 = OSY;
+        sa.os2 = OSX;
+        sa.nt0 = p->ntile[0];
+        sa.nt1 = p->ntile[1];
+        sa.nt2 = p->ntile[2];
+        sa.beta = p->beta;
+        sa.K = std::max(64, std::min(256, (int)((48 * 1024) / (sa.ncc * sizeof(float2)))));
+        const int cpt = (sa.ncc + 3) / 4;
+        const unsigned nt = (unsigned)p->ntiles;
+        if (cpt <= 1) TR_TRY(launch_spread_t<1>(sa, nt, st));
+        else if (cpt <= 4) TR_TRY(launch_spread_t<4>(sa, nt, st));
+        else if (cpt <= 8) TR_TRY(launch_spread_t<8>(sa, nt, st));
+        else if (cpt <= 16) TR_TRY(launch_spread_t<16>(sa, nt, st));
+        else if (cpt <= 24) TR_TRY(launch_spread_t<24>(sa, nt, st));
+        else TR_TRY(launch_spread_t<32>(sa, nt, st));
+    }
+    // z pass (inverse, crop to Z): [1][OSZ -> Z][OSY * OSX * ncol]
+    TR_TRY(launch_line(p, 0, p->bufA, p->bufB, 1, (int64_t)OSY * OSX * ncol, OSZ, Z, 0, p->ax[0].pad, true, st));
+    // y pass (inverse, crop to Y): [Z][OSY -> Y][OSX * ncol]
+    TR_TRY(launch_line(p, 1, p->bufB, p->bufA, Z, (int64_t)OSX * ncol, OSY, Y, 0, p->ax[1].pad, true, st));
+    // x pass with coil combine
+    AdjXArgs aa;
+    aa.in = p->bufA;
+    aa.ncol = ncol;
+    aa.maps = maps;
+    aa.C = C;
+    aa.cc = coils_per_cta(C);
+    aa.rows = std::max(1, 16 / aa.cc);
+    aa.Z = Z;
+    aa.Y = Y;
+    aa.X = X;
+    aa.OSX = OSX;
+    aa.h = p->ax[2].h;
+    aa.pad = p->ax[2].pad;
+    aa.apz = p->ax[0].apod;
+    aa.apy = p->ax[1].apod;
+    aa.apx = p->ax[2].apod;
+    aa.scale = p->adj_scale;
+    aa.tw = p->ax[2].twiddle;
+    aa.S = stages_of(p->ax[2]);
+    aa.img = images;
+    aa.img_stride = img_stride;
+    aa.accumulate = 0;
+    const int W = aa.rows * aa.cc;
+    const size_t smem = fft_smem_bytes(OSX, W) + (size_t)aa.rows * X * sizeof(float2);
+    TR_TRY(set_smem_limit((const void*)k_adj_x, smem));
+    dim3 grid((unsigned)((Z * Y + aa.rows - 1) / aa.rows), (unsigned)n_img);
+    k_adj_x<<<grid, 256, smem, st>>>(aa);
+    TR_CHECK_LAUNCH();
+    return TR_OK;
+}
+
+static double apod_value(int i, int n, int L, int width, double beta) {
+    const double t = M_PI * width * (double)(i - n / 2) / (double)L;
+    const double r = std::sqrt(beta * beta - t * t);
+    return r / std::sinh(r);
+}
+
+static void plan_free(tr_plan* p) {
+    if (!p) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(p->device);
+    pdhg_destroy(p);
+    wavelet_destroy(p);
+    for (auto& a : p->ax) {
+        cudaFree(a.twiddle);
+        cudaFree(a.apod);
+    }
+    cudaFree(p->ks);
+    cudaFree(p->perm);
+    cudaFree(p->tile_start);
+    cudaFree(p->tile_order);
+    cudaFree(p->maps);
+    cudaFree(p->bufA);
+    cudaFree(p->bufB);
+    cudaFree(p->one_in);
+    cudaFree(p->one_out);
+    cudaFree(p->partials);
+    cudaFree(p->tol_dev);
+    if (p->tol_host) cudaFreeHost(p->tol_host);
+    cudaSetDevice(cur);
+    delete p;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
+    if (!d || !out) return fail(TR_ERR_INVALID_ARG, "tr_plan_create: null argument");
+    *out = nullptr;
+    for (int i = 0; i < 3; ++i)
+        if (d->img_shape[i] < 10)
+            return fail(TR_ERR_INVALID_ARG, "img_shape must be three values >= 10 (z, y, x)");
+    if (d->n_bins < 1 || !d->bin_counts) return fail(TR_ERR_INVALID_ARG, "at least one trajectory bin is required");
+    if (d->n_coils < 1 || d->n_echoes < 1) return fail(TR_ERR_INVALID_ARG, "n_coils and n_echoes must be >= 1");
+    if (std::fabs(d->oversamp - 1.25f) > 1e-6f || d->width != 4)
+        return fail(TR_ERR_UNSUPPORTED, "only oversamp = 1.25 and width = 4 (the reference's SigPy defaults) are supported");
+    int ndev = 0;
+    TR_CUDA(cudaGetDeviceCount(&ndev));
+    if (d->device < 0 || d->device >= ndev) return fail(TR_ERR_INVALID_ARG, "invalid CUDA device ordinal");
+    DeviceGuard guard(d->device);
+
+    tr_plan* p = new tr_plan();
+    p->device = d->device;
+    p->C = d->n_coils;
+    p->E = d->n_echoes;
+    p->B = d->n_bins;
+    p->width = d->width;
+    const double beta = M_PI * std::sqrt(std::pow(d->width / (double)d->oversamp * (d->oversamp - 0.5), 2.0) - 0.8);
+    p->beta = (float)beta;
+    double N = 1.0;
+    for (int i = 0; i < 3; ++i) {
+        p->n[i] = d->img_shape[i];
+        p->os[i] = (int)std::ceil((double)d->oversamp * d->img_shape[i]);
+        N *= p->n[i];
+    }
+    p->fwd_scale = (float)(1.0 / (std::sqrt(N) * std::pow((double)d->width, 3)));
+    p->adj_scale = p->fwd_scale;
+    auto bad = [&](tr_status code, const std::string& m) {
+        plan_free(p);
+        return fail(code, m);
+    };
+    for (int i = 0; i < 3; ++i) {
+        FftAxis& A = p->ax[i];
+        A.n = p->n[i];
+        A.L = p->os[i];
+        A.h = A.L / 2;
+        A.pad = A.L / 2 - A.n / 2;
+        if (A.L > kMaxFftLen || !factor_radices(A.L, A.radix, &A.nstages))
+            return bad(TR_ERR_UNSUPPORTED, "oversampled length " + std::to_string(A.L) +
+                                           " must factor into 2, 3, 5, 7 and be <= 1024");
+        std::vector<float2> tw(A.L);
+        for (int k = 0; k < A.L; ++k) {
+            const double ang = -2.0 * M_PI * (double)k / (double)A.L;
+            tw[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+        }
+        std::vector<float> ap(A.n);
+        for (int k = 0; k < A.n; ++k) ap[k] = (float)apod_value(k, A.n, A.L, d->width, beta);
+        if (cudaMalloc(&A.twiddle, A.L * sizeof(float2)) != cudaSuccess ||
+            cudaMalloc(&A.apod, A.n * sizeof(float)) != cudaSuccess)
+            return bad(TR_ERR_OOM, "allocation of FFT tables failed");
+        cudaMemcpy(A.twiddle, tw.data(), A.L * sizeof(float2), cudaMemcpyHostToDevice);
+        cudaMemcpy(A.apod, ap.data(), A.n * sizeof(float), cudaMemcpyHostToDevice);
+        p->ntile[i] = (A.L + kTile - 1) / kTile;
+    }
+    p->ntiles = (int64_t)p->ntile[0] * p->ntile[1] * p->ntile[2];
+
+    // bins
+    p->bins.resize(d->n_bins);
+    int64_t off = 0;
+    for (int b = 0; b < d->n_bins; ++b) {
+        if (d->bin_counts[b] < 0 || d->bin_counts[b] > (int64_t)INT32_MAX)
+            return bad(TR_ERR_INVALID_ARG, "bin sample counts must be in [0, 2^31)");
+        p->bins[b].offset = off;
+        p->bins[b].count = d->bin_counts[b];
+        off += d->bin_counts[b];
+    }
+    p->total = off;
+    if (off > 0 && !d->coords) return bad(TR_ERR_INVALID_ARG, "coords is null");
+    p->has_dcf = d->dcf != nullptr;
+
+    // scale coordinates exactly as the reference (float32 multiply, then add)
+    std::vector<float4> ks_sorted((size_t)std::max<int64_t>(off, 1));
+    std::vector<int32_t> perm((size_t)std::max<int64_t>(off, 1));
+    std::vector<int32_t> tstart((size_t)(p->ntiles + 1) * d->n_bins);
+    std::vector<int32_t> torder((size_t)p->ntiles * d->n_bins);
+    float scale[3], shift[3];
+    for (int i = 0; i < 3; ++i) {
+        scale[i] = (float)((double)p->os[i] / (double)p->n[i]);
+        shift[i] = (float)(p->os[i] / 2);
+    }
+    std::vector<int32_t> key;
+    std::vector<float4> kscaled;
+    for (int b = 0; b < d->n_bins; ++b) {
+        const int64_t M = p->bins[b].count, o = p->bins[b].offset;
+        key.assign((size_t)M, 0);
+        kscaled.assign((size_t)M, make_float4(0, 0, 0, 0));
+        for (int64_t m = 0; m < M; ++m) {
+            float kc[3];
+            for (int i = 0; i < 3; ++i) {
+                volatile float t = d->coords[(o + m) * 3 + i] * scale[i];
+                kc[i] = t + shift[i];
+                if (!std::isfinite(kc[i])) return bad(TR_ERR_INVALID_ARG, "coordinates must be finite");
+            }
+            const float w = d->dcf ? d->dcf[o + m] : 1.0f;
+            kscaled[(size_t)m] = make_float4(kc[0], kc[1], kc[2], w);
+            int tcoord[3];
+            for (int i = 0; i < 3; ++i) {
+                long long f = (long long)std::floor((double)kc[i]);
+                long long r = f % p->os[i];
+                if (r < 0) r += p->os[i];
+                tcoord[i] = (int)(r / kTile);
+            }
+            key[(size_t)m] = (tcoord[0] * p->ntile[1] + tcoord[1]) * p->ntile[2] + tcoord[2];
+        }
+        // stable counting sort by tile
+        int32_t* ts = &tstart[(size_t)b * (p->ntiles + 1)];
+        std::fill(ts, ts + p->ntiles + 1, 0);
+        for (int64_t m = 0; m < M; ++m) ts[key[(size_t)m] + 1]++;
+        for (int64_t t = 0; t < p->ntiles; ++t) ts[t + 1] += ts[t];
+        std::vector<int32_t> fillp(ts, ts + p->ntiles);
+        for (int64_t m = 0; m < M; ++m) {
+            const int32_t pos = fillp[key[(size_t)m]]++;
+            perm[(size_t)(o + pos)] = (int32_t)m;
+            ks_sorted[(size_t)(o + pos)] = kscaled[(size_t)m];
+        }
+        // work queue: tiles ordered by candidate count (27 neighbours), heaviest first
+        std::vector<std::pair<int64_t, int32_t>> work((size_t)p->ntiles);
+        for (int tz = 0; tz < p->ntile[0]; ++tz)
+            for (int ty = 0; ty < p->ntile[1]; ++ty)
+                for (int tx = 0; tx < p->ntile[2]; ++tx) {
+                    int64_t cnt = 0;
+                    for (int dz = -1; dz <= 1; ++dz)
+                        for (int dy = -1; dy <= 1; ++dy)
+                            for (int dx = -1; dx <= 1; ++dx) {
+                                int nz = (tz + dz + p->ntile[0]) % p->ntile[0];
+                                int ny = (ty + dy + p->ntile[1]) % p->ntile[1];
+                                int nx = (tx + dx + p->ntile[2]) % p->ntile[2];
+                                int id = (nz * p->ntile[1] + ny) * p->ntile[2] + nx;
+                                cnt += ts[id + 1] - ts[id];
+                            }
+                    const int32_t id = (tz * p->ntile[1] + ty) * p->ntile[2] + tx;
+                    work[(size_t)id] = {-cnt, id};
+                }
+        std::stable_sort(work.begin(), work.end(),
+                         [](const std::pair<int64_t, int32_t>& x, const std::pair<int64_t, int32_t>& y) {
+                             return x.first < y.first;
+                         });
+        for (int64_t t = 0; t < p->ntiles; ++t) torder[(size_t)b * p->ntiles + t] = work[(size_t)t].second;
+    }
+    const size_t nks = (size_t)std::max<int64_t>(off, 1);
+    if (cudaMalloc(&p->ks, nks * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc(&p->perm, nks * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&p->tile_start, tstart.size() * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&p->tile_order, torder.size() * sizeof(int32_t)) != cudaSuccess)
+        return bad(TR_ERR_OOM, "allocation of the sorted trajectory failed");
+    TR_CUDA(cudaMemcpy(p->ks, ks_sorted.data(), nks * sizeof(float4), cudaMemcpyHostToDevice));
+    TR_CUDA(cudaMemcpy(p->perm, perm.data(), nks * sizeof(int32_t), cudaMemcpyHostToDevice));
+    TR_CUDA(cudaMemcpy(p->tile_start, tstart.data(), tstart.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    TR_CUDA(cudaMemcpy(p->tile_order, torder.data(), torder.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    if (cudaMalloc(&p->tol_dev, 4 * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&p->tol_host, 4 * sizeof(double)) != cudaSuccess)
+        return bad(TR_ERR_OOM, "allocation of reduction scalars failed");
+    p->workspace_bytes = (int64_t)(nks * (sizeof(float4) + sizeof(int32_t)) +
+                                   (tstart.size() + torder.size()) * sizeof(int32_t));
+    TR_TRY(wavelet_prepare(p));
+    *out = p;
+    return TR_OK;
+}
+
+}  // namespace tr
+
+using namespace tr;
+
+extern "C" {
+
+const char* tr_last_error_string(void) { return g_last_error.c_str(); }
+
+tr_status tr_plan_create(const tr_plan_desc* desc, tr_plan** out) {
+    try {
+        return plan_create_impl(desc, out);
+    } catch (const std::exception& e) {
+        return fail(TR_ERR_OOM, std::string("tr_plan_create: ") + e.what());
+    }
+}
+
+tr_status tr_plan_destroy(tr_plan* plan) {
+    if (!plan) return TR_OK;
+    plan_free(plan);
+    return TR_OK;
+}
+
+tr_status tr_plan_info(const tr_plan* p, tr_plan_info_t* info) {
+    if (!p || !info) return fail(TR_ERR_INVALID_ARG, "tr_plan_info: null argument");
+    for (int i = 0; i < 3; ++i) info->os_shape[i] = p->os[i];
+    info->total_samples = p->total;
+    info->workspace_bytes = p->workspace_bytes;
+    info->fft_line_width = p->line_width;
+    info->wavelet_levels = 0;
+    info->wavelet_coeffs = 0;
+    wavelet_info(p, &info->wavelet_levels, &info->wavelet_coeffs);
+    return TR_OK;
+}
+
+tr_status tr_plan_bin_offset(const tr_plan* p, int32_t bin, int64_t* offset, int64_t* count) {
+    if (!p) return fail(TR_ERR_INVALID_ARG, "null plan");
+    if (bin < 0 || bin >= p->B)
+        return fail(TR_ERR_INVALID_ARG, "bin_index " + std::to_string(bin) + " is outside [0, " +
+                                            std::to_string(p->B) + ").");
+    if (offset) *offset = p->bins[bin].offset;
+    if (count) *count = p->bins[bin].count;
+    return TR_OK;
+}
+
+tr_status tr_plan_set_maps(tr_plan* p, const void* mps, void* stream) {
+    if (!p || !mps) return fail(TR_ERR_INVALID_ARG, "tr_plan_set_maps: null argument");
+    DeviceGuard g(p->device);
+    const int64_t N = (int64_t)p->n[0] * p->n[1] * p->n[2];
+    if (!p->maps) {
+        TR_CUDA(cudaMalloc(&p->maps, (size_t)N * p->C * sizeof(float2)));
+        p->workspace_bytes += N * p->C * (int64_t)sizeof(float2);
+    }
+    const int64_t tot = N * p->C;
+    k_interleave_maps<<<(unsigned)((tot + 255) / 256), 256, 0, (cudaStream_t)stream>>>((const float2*)mps, p->maps,
+                                                                                        N, p->C);
+    TR_CHECK_LAUNCH();
+    return TR_OK;
+}
+
+tr_status tr_plan_sort_kspace(tr_plan* p, int32_t bin, const void* ext, void* internal, int32_t ncol,
+                              void* stream) {
+    TR_TRY(tr_plan_bin_offset(p, bin, nullptr, nullptr));
+    if (!ext || !internal || ncol < 1) return fail(TR_ERR_INVALID_ARG, "tr_plan_sort_kspace: bad argument");
+    DeviceGuard g(p->device);
+    const Bin& b = p->bins[bin];
+    const int64_t n = b.count * ncol;
+    if (n == 0) return TR_OK;
+    k_sort_ksp<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        (const float2*)ext, (float2*)internal, p->perm + b.offset, b.count, ncol);
+    TR_CHECK_LAUNCH();
+    return TR_OK;
+}
+
+tr_status tr_plan_unsort_kspace(tr_plan* p, int32_t bin, const void* internal, void* ext, int32_t ncol,
+                                void* stream) {
+    TR_TRY(tr_plan_bin_offset(p, bin, nullptr, nullptr));
+    if (!ext || !internal || ncol < 1) return fail(TR_ERR_INVALID_ARG, "tr_plan_unsort_kspace: bad argument");
+    DeviceGuard g(p->device);
+    const Bin& b = p->bins[bin];
+    const int64_t n = b.count * ncol;
+    if (n == 0) return TR_OK;
+    k_unsort_ksp<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        (const float2*)internal, (float2*)ext, p->perm + b.offset, b.count, ncol);
+    TR_CHECK_LAUNCH();
+    return TR_OK;
+}
+
+static tr_status ensure_one(tr_plan* p) {
+    size_t need = (size_t)std::max<int64_t>(1, 0);
+    for (auto& b : p->bins) need = std::max(need, (size_t)b.count);
+    if (p->one_in && p->one_elems >= need) return TR_OK;
+    cudaFree(p->one_in);
+    cudaFree(p->one_out);
+    p->one_in = p->one_out = nullptr;
+    TR_CUDA(cudaMalloc(&p->one_in, need * sizeof(float2)));
+    TR_CUDA(cudaMalloc(&p->one_out, need * sizeof(float2)));
+    p->one_elems = need;
+    return TR_OK;
+}
+
+tr_status tr_nufft_forward(tr_plan* p, int32_t bin, const void* image, void* ksp, void* stream) {
+    TR_TRY(tr_plan_bin_offset(p, bin, nullptr, nullptr));
+    if (!image || !ksp) return fail(TR_ERR_INVALID_ARG, "tr_nufft_forward: null pointer");
+    DeviceGuard g(p->device);
+    TR_TRY(ensure_one(p));
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t N = (int64_t)p->n[0] * p->n[1] * p->n[2];
+    TR_TRY(nufft_forward_cols(p, bin, (const float2*)image, N, 1, nullptr, 1, kInterpStore, 0.f, nullptr,
+                              p->one_out, st));
+    return tr_plan_unsort_kspace(p, bin, p->one_out, ksp, 1, stream);
+}
+
+tr_status tr_nufft_adjoint(tr_plan* p, int32_t bin, const void* ksp, void* image, void* stream) {
+    TR_TRY(tr_plan_bin_offset(p, bin, nullptr, nullptr));
+    if (!image || !ksp) return fail(TR_ERR_INVALID_ARG, "tr_nufft_adjoint: null pointer");
+    DeviceGuard g(p->device);
+    TR_TRY(ensure_one(p));
+    cudaStream_t st = (cudaStream_t)stream;
+    TR_TRY(tr_plan_sort_kspace(p, bin, ksp, p->one_in, 1, stream));
+    const int64_t N = (int64_t)p->n[0] * p->n[1] * p->n[2];
+    return nufft_adjoint_cols(p, bin, p->one_in, 1, nullptr, 1, false, (float2*)image, N, st);
+}
+
+tr_status tr_nufft_forward_bin(tr_plan* p, int32_t bin, const void* images, void* ksp_internal, void* stream) {
+    TR_TRY(tr_plan_bin_offset(p, bin, nullptr, nullptr));
+    if (!images || !ksp_internal) return fail(TR_ERR_INVALID_ARG, "tr_nufft_forward_bin: null pointer");
+    if (!p->maps) return fail(TR_ERR_INVALID_ARG, "coil maps not set (tr_plan_set_maps)");
+    DeviceGuard g(p->device);
+    const int64_t N = (int64_t)p->n[0] * p->n[1] * p->n[2];
+    return nufft_forward_cols(p, bin, (const float2*)images, N, p->E, p->maps, p->C, kInterpStore, 0.f, nullptr,
+                              (float2*)ksp_internal, (cudaStream_t)stream);
+}
+
+tr_status tr_nufft_adjoint_bin(tr_plan* p, int32_t bin, const void* ksp_internal, int32_t use_dcf, void* images,
+                               void* stream) {
+    TR_TRY(tr_plan_bin_offset(p, bin, nullptr, nullptr));
+    if (!images || !ksp_internal) return fail(TR_ERR_INVALID_ARG, "tr_nufft_adjoint_bin: null pointer");
+    if (!p->maps) return fail(TR_ERR_INVALID_ARG, "coil maps not set (tr_plan_set_maps)");
+    DeviceGuard g(p->device);
+    const int64_t N = (int64_t)p->n[0] * p->n[1] * p->n[2];
+    return nufft_adjoint_cols(p, bin, (const float2*)ksp_internal, p->E, p->maps, p->C, use_dcf != 0,
+                              (float2*)images, N, (cudaStream_t)stream);
+}
+
+}  // extern "C"

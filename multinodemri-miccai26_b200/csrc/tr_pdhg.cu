@@ -1,0 +1,521 @@
+// PDHG iterations for TVM / TVME / TVMW on one B200.
+//
+// One iteration (the reference's order, single device, every ghost a global edge):
+//   1. data dual   q_b <- (q_b + sigma (F_b(u_bar S) - y_b)) / (1 + sigma)      [NUFFT forward, fused]
+//   2. TV duals    one pass over (B, E, Z, Y, X): motion (L1 or L2 over echoes),
+//                  TVME echo-spatial isotropic TV, TVMW db1 echo wavelet       [k_dual]
+//      TVMW       db6 spatial wavelet dual with the L-inf projection         [tr_wavelet.cu]
+//   3. data grad   g_b = sum_c conj(S_c) F_b^H(dcf q_b)                        [NUFFT adjoint, fused]
+//      TVMW       w2adj = waverec3(p_w2)
+//   4. primal      u <- u - tau(...), u_bar <- 2 u_new - u_old, FP64 partial
+//                  sums of the stopping tolerance                              [k_primal]
+//   5. tolerance   fixed-order FP64 reduction of the partial sums             [k_tol_finalize]
+//
+// Reference: tvm.py:227-380, tvme.py:208-482, tvmw.py:385-685 (iteration),
+// tvm.py:406-472, tvme.py:512-557, tvmw.py:716-773 (tolerance and stop).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "tr_internal.cuh"
+
+namespace tr {
+
+struct PdhgGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    tr_pdhg_state state;
+    tr_pdhg_params params;
+    cudaStream_t stream = nullptr;
+};
+
+void pdhg_destroy(tr_plan* p) {
+    if (!p->graph) return;
+    if (p->graph->exec) cudaGraphExecDestroy(p->graph->exec);
+    if (p->graph->graph) cudaGraphDestroy(p->graph->graph);
+    delete p->graph;
+    p->graph = nullptr;
+}
+
+struct PdArgs {
+    const float2* ubar;
+    float2* u;
+    float2* ubar_out;
+    const float2* g;
+    const float2* w2adj;
+    float2* pm;
+    float2* pex;
+    float2* pey;
+    float2* pez;
+    float2* pw1;
+    int alg, l2;
+    int B, E, Z, Y, X;
+    int64_t N;
+    float sigma, tau, lam_m, lam_e, lam_w1;
+    double* partials;
+};
+
+__device__ __forceinline__ float2 cdivr(float2 v, float d) { return make_float2(v.x / d, v.y / d); }
+__device__ __forceinline__ float cabsf(float2 v) { return sqrtf(v.x * v.x + v.y * v.y); }
+
+// ------------------------------------------------------------------ duals
+__global__ void __launch_bounds__(256) k_dual(PdArgs a) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)a.B * a.N) return;
+    const int b = (int)(t / a.N);
+    const int64_t v = t - (int64_t)b * a.N;
+    const int YX = a.Y * a.X;
+    const int z = (int)(v / YX);
+    const int rem = (int)(v - (int64_t)z * YX);
+    const int y = rem / a.X;
+    const int x = rem - y * a.X;
+    const int64_t EN = (int64_t)a.E * a.N;
+    const float2* ub = a.ubar + (int64_t)b * EN;
+    const float2* ubn = (b + 1 < a.B) ? ub + EN : nullptr;
+    const float sig = a.sigma;
+    float s2 = 0.f;
+    for (int e = 0; e < a.E; ++e) {
+        const int64_t o = (int64_t)b * EN + (int64_t)e * a.N + v;
+        const float2 u0 = ub[(int64_t)e * a.N + v];
+        // motion: p_m += sigma (u_bar[b+1] - u_bar[b]) (0 at the last bin)
+        float2 dm = make_float2(0.f, 0.f);
+        if (ubn) dm = csub(ubn[(int64_t)e * a.N + v], u0);
+        float2 pm = a.pm[o];
+        pm = make_float2(pm.x + sig * dm.x, pm.y + sig * dm.y);
+        if (!a.l2) {
+            const float den = fmaxf(1.0f, cabsf(pm) / a.lam_m);
+            pm = cdivr(pm, den);
+        } else {
+            const float m = cabsf(pm);
+            s2 += m * m;
+        }
+        a.pm[o] = pm;
+        if (a.alg == TR_ALG_TVME) {
+            float2 gx = make_float2(0.f, 0.f), gy = gx, gz = gx;
+            if (e + 1 < a.E) {
+                const float2* u_e = ub + (int64_t)e * a.N;
+                const float2* u_n = u_e + a.N;
+                const float2 d0 = csub(u_n[v], u_e[v]);
+                if (x + 1 < a.X) gx = csub(csub(u_n[v + 1], u_e[v + 1]), d0);
+                if (y + 1 < a.Y) gy = csub(csub(u_n[v + a.X], u_e[v + a.X]), d0);
+                if (z + 1 < a.Z) gz = csub(csub(u_n[v + YX], u_e[v + YX]), d0);
+            }
+            float2 px = a.pex[o], py = a.pey[o], pz = a.pez[o];
+            px = make_float2(px.x + sig * gx.x, px.y + sig * gx.y);
+            py = make_float2(py.x + sig * gy.x, py.y + sig * gy.y);
+            pz = make_float2(pz.x + sig * gz.x, pz.y + sig * gz.y);
+            const float ax = cabsf(px), ay = cabsf(py), az = cabsf(pz);
+            const float mag = sqrtf(ax * ax + ay * ay + az * az);
+            const float den = fmaxf(1.0f, mag / a.lam_e);
+            a.pex[o] = cdivr(px, den);
+            a.pey[o] = cdivr(py, den);
+            a.pez[o] = cdivr(pz, den);
+        } else if (a.alg == TR_ALG_TVMW) {
+            // db1 along echo: even e: (u_e + u_{e+1})/sqrt2 ; odd e: (u_e - u_{e-1})/sqrt2
+            const float s = 0.70710678118654752f;
+            float2 w;
+            if ((e & 1) == 0) {
+                float2 x1 = (e + 1 < a.E) ? ub[(int64_t)(e + 1) * a.N + v] : make_float2(0.f, 0.f);
+                w = cscale(cadd(u0, x1), s);
+            } else {
+                const float2 xm = ub[(int64_t)(e - 1) * a.N + v];
+                w = cscale(cadd(make_float2(-xm.x, -xm.y), u0), s);
+            }
+            float2 pw = a.pw1[o];
+            pw = make_float2(pw.x + sig * w.x, pw.y + sig * w.y);
+            if (a.lam_w1 > 0.f) {
+                const float den = fmaxf(1.0f, cabsf(pw) / a.lam_w1);
+                pw = cdivr(pw, den);
+            } else {
+                pw = make_float2(0.f, 0.f);
+            }
+            a.pw1[o] = pw;
+        }
+    }
+    if (a.l2) {
+        const float den = fmaxf(1.0f, sqrtf(s2) / a.lam_m);
+        for (int e = 0; e < a.E; ++e) {
+            const int64_t o = (int64_t)b * EN + (int64_t)e * a.N + v;
+            a.pm[o] = cdivr(a.pm[o], den);
+        }
+    }
+}
+
+// Exact transpose of the zero-last-row forward difference along one axis:
+// d[i] = -p[i] (i < n-1) + p[i-1] (i >= 1).
+__device__ __forceinline__ float2 back_diff(const float2* p, int64_t v, int64_t stride, int i, int n) {
+    float2 d = make_float2(0.f, 0.f);
+    if (i >= 1) d = p[v - stride];
+    if (i < n - 1) d = csub(d, p[v]);
+    return d;
+}
+
+__device__ __forceinline__ void block_reduce_partials(double num, double den, double* partials) {
+    __shared__ double sn[8], sd[8];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        num += __shfl_down_sync(0xffffffffu, num, off);
+        den += __shfl_down_sync(0xffffffffu, den, off);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        sn[warp] = num;
+        sd[warp] = den;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            a += sn[w];
+            b += sd[w];
+        }
+        partials[2 * blockIdx.x] = a;
+        partials[2 * blockIdx.x + 1] = b;
+    }
+}
+
+// ------------------------------------------------------------------ primal + extrapolation + tolerance
+__global__ void __launch_bounds__(256) k_primal(PdArgs a) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double num = 0.0, den = 0.0;
+    if (t < (int64_t)a.B * a.N) {
+        const int b = (int)(t / a.N);
+        const int64_t v = t - (int64_t)b * a.N;
+        const int YX = a.Y * a.X;
+        const int z = (int)(v / YX);
+        const int rem = (int)(v - (int64_t)z * YX);
+        const int y = rem / a.X;
+        const int x = rem - y * a.X;
+        const int64_t EN = (int64_t)a.E * a.N;
+        const float tau = a.tau;
+        float2 divprev = make_float2(0.f, 0.f);
+        for (int e = 0; e < a.E; ++e) {
+            const int64_t o = (int64_t)b * EN + (int64_t)e * a.N + v;
+            const float2 uo = a.u[o];
+            const float2 g = a.g[o];
+            float2 un;
+            if (a.alg == TR_ALG_TVME) {
+                // divp_m = D_m^T p_m  (tvme.py:421-437)
+                float2 dm = make_float2(0.f, 0.f);
+                if (a.B > 1) {
+                    if (b == 0) dm = make_float2(-a.pm[o].x, -a.pm[o].y);
+                    else if (b == a.B - 1) dm = a.pm[o - EN];
+                    else dm = csub(a.pm[o - EN], a.pm[o]);
+                }
+                // divp = dxb(p_ex) + dyb(p_ey) + dzb(p_ez) at (b, e)
+                const float2 dx = back_diff(a.pex + (o - v), v, 1, x, a.X);
+                const float2 dy = back_diff(a.pey + (o - v), v, a.X, y, a.Y);
+                const float2 dz = back_diff(a.pez + (o - v), v, YX, z, a.Z);
+                const float2 divc = cadd(cadd(dx, dy), dz);
+                // divp_e = D_e^T divp  (tvme.py:361-363, :444-454)
+                float2 de;
+                if (e == 0) de = make_float2(-divc.x, -divc.y);
+                else if (e == a.E - 1) de = divprev;
+                else de = csub(divprev, divc);
+                divprev = divc;
+                un = make_float2(uo.x - tau * dm.x, uo.y - tau * dm.y);
+                un = make_float2(un.x - tau * de.x, un.y - tau * de.y);
+                un = make_float2(un.x - tau * g.x, un.y - tau * g.y);
+            } else if (a.alg == TR_ALG_TVM) {
+                // divergence = p[b] - p[b-1] with the reference's edges (tvm.py:342-357)
+                float2 dv;
+                if (a.B == 1) dv = make_float2(0.f, 0.f);
+                else if (b == 0) dv = a.pm[o];
+                else if (b == a.B - 1) dv = make_float2(-a.pm[o - EN].x, -a.pm[o - EN].y);
+                else dv = csub(a.pm[o], a.pm[o - EN]);
+                const float2 r = csub(g, dv);
+                un = make_float2(uo.x + (-tau) * r.x, uo.y + (-tau) * r.y);
+            } else {
+                // TVMW: u_tmp -= tau (g - divp_m + divp_w1 + divp_w2)  (tvmw.py:662-681)
+                float2 dvm = (b == 0) ? a.pm[o] : csub(a.pm[o], a.pm[o - EN]);
+                const float s = 0.70710678118654752f;
+                float2 w1;
+                if ((e & 1) == 0) {
+                    const float2 dn = (e + 1 < a.E) ? a.pw1[o + a.N] : make_float2(0.f, 0.f);
+                    w1 = cscale(csub(a.pw1[o], dn), s);
+                } else {
+                    w1 = cscale(cadd(a.pw1[o - a.N], a.pw1[o]), s);
+                }
+                const float2 r = cadd(cadd(csub(g, dvm), w1), a.w2adj[o]);
+                un = make_float2(uo.x - tau * r.x, uo.y - tau * r.y);
+            }
+            const float2 ubn = make_float2(2.0f * un.x - uo.x, 2.0f * un.y - uo.y);
+            a.u[o] = un;
+            if (a.alg == TR_ALG_TVMW) {
+                // tolerance on u_bar: ||u_bar_prev - u_bar_new|| / ||u_bar_prev|| (tvmw.py:721-769)
+                const float2 up = a.ubar[o];
+                const double ddx = (double)up.x - (double)ubn.x, ddy = (double)up.y - (double)ubn.y;
+                num += ddx * ddx + ddy * ddy;
+                den += (double)up.x * up.x + (double)up.y * up.y;
+            } else {
+                // tolerance on u: ||u_new - u_old|| / ||u_new|| (tvme.py:518-551)
+                const double ddx = (double)un.x - (double)uo.x, ddy = (double)un.y - (double)uo.y;
+                num += ddx * ddx + ddy * ddy;
+                den += (double)un.x * un.x + (double)un.y * un.y;
+            }
+            a.ubar_out[o] = ubn;
+        }
+    }
+    block_reduce_partials(num, den, a.partials);
+}
+
+__global__ void k_tol_finalize(const double* __restrict__ partials, int n, double* out) {
+    __shared__ double sn[256], sd[256];
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        a += partials[2 * i];
+        b += partials[2 * i + 1];
+    }
+    sn[threadIdx.x] = a;
+    sd[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) {
+            sn[threadIdx.x] += sn[threadIdx.x + s];
+            sd[threadIdx.x] += sd[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = sn[0];
+        out[1] = sd[0];
+    }
+}
+
+// ------------------------------------------------------------------ driver
+static tr_status validate(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_params* q) {
+    if (!p || !s || !q) return fail(TR_ERR_INVALID_ARG, "tr_pdhg_run: null argument");
+    if (!p->maps) return fail(TR_ERR_INVALID_ARG, "coil maps not set (tr_plan_set_maps)");
+    if (!s->u || !s->u_bar || !s->p_m || !s->q || !s->y || !s->g)
+        return fail(TR_ERR_INVALID_ARG, "state u, u_bar, p_m, q, y and g are required");
+    if (q->algorithm == TR_ALG_TVME && (!s->p_ex || !s->p_ey || !s->p_ez))
+        return fail(TR_ERR_INVALID_ARG, "TVME needs p_ex, p_ey, p_ez");
+    if (q->algorithm == TR_ALG_TVMW && (!s->p_w1 || !s->p_w2 || !s->w2adj))
+        return fail(TR_ERR_INVALID_ARG, "TVMW needs p_w1, p_w2, w2adj");
+    if (q->algorithm < 0 || q->algorithm > 2) return fail(TR_ERR_INVALID_ARG, "unknown algorithm");
+    if (!(q->sigma > 0.f) || !(q->tau > 0.f)) return fail(TR_ERR_INVALID_ARG, "sigma and tau must be positive");
+    return TR_OK;
+}
+
+static tr_status enqueue_iteration(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_params* q, cudaStream_t st) {
+    const int64_t N = (int64_t)p->n[0] * p->n[1] * p->n[2];
+    const int64_t EN = (int64_t)p->E * N;
+    const int ncol = p->E * p->C;
+    float2* u = (float2*)s->u;
+    float2* ubar = (float2*)s->u_bar;
+    float2* qd = (float2*)s->q;
+    const float2* y = (const float2*)s->y;
+    float2* g = (float2*)s->g;
+    // TVMW: the spatial-wavelet dual reads u_bar before anything changes it
+    if (q->algorithm == TR_ALG_TVMW)
+        TR_TRY(wavelet_dual(p, ubar, (float2*)s->p_w2, q->sigma, q->lam_w2, st));
+    // 1. data dual
+    for (int b = 0; b < p->B; ++b) {
+        const int64_t off = p->bins[b].offset * ncol;
+        TR_TRY(nufft_forward_cols(p, b, ubar + (int64_t)b * EN, N, p->E, p->maps, p->C, kInterpDualProx, q->sigma,
+                                  y + off, qd + off, st));
+    }
+    // 2. TV / W1 duals
+    PdArgs a;
+    memset(&a, 0, sizeof(a));
+    a.ubar = ubar;
+    a.u = u;
+    a.ubar_out = ubar;
+    a.g = g;
+    a.w2adj = (const float2*)s->w2adj;
+    a.pm = (float2*)s->p_m;
+    a.pex = (float2*)s->p_ex;
+    a.pey = (float2*)s->p_ey;
+    a.pez = (float2*)s->p_ez;
+    a.pw1 = (float2*)s->p_w1;
+    a.alg = q->algorithm;
+    a.l2 = q->l2_coupling;
+    a.B = p->B;
+    a.E = p->E;
+    a.Z = p->n[0];
+    a.Y = p->n[1];
+    a.X = p->n[2];
+    a.N = N;
+    a.sigma = q->sigma;
+    a.tau = q->tau;
+    a.lam_m = q->lam_m;
+    a.lam_e = q->lam_e;
+    a.lam_w1 = q->lam_w1;
+    const int64_t nthr = (int64_t)p->B * N;
+    const unsigned blocks = (unsigned)((nthr + 255) / 256);
+    k_dual<<<blocks, 256, 0, st>>>(a);
+    TR_CHECK_LAUNCH();
+    // 3. coil-combined, density-weighted adjoint
+    for (int b = 0; b < p->B; ++b) {
+        const int64_t off = p->bins[b].offset * ncol;
+        TR_TRY(nufft_adjoint_cols(p, b, qd + off, p->E, p->maps, p->C, true, g + (int64_t)b * EN, N, st));
+    }
+    if (q->algorithm == TR_ALG_TVMW) TR_TRY(wavelet_adjoint(p, (const float2*)s->p_w2, (float2*)s->w2adj, st));
+    // 4. primal, extrapolation, tolerance partials
+    if (!p->partials || p->npartials < (int)blocks) {
+        cudaFree(p->partials);
+        p->partials = nullptr;
+        TR_CUDA(cudaMalloc(&p->partials, (size_t)blocks * 2 * sizeof(double)));
+        p->npartials = (int)blocks;
+    }
+    a.partials = p->partials;
+    k_primal<<<blocks, 256, 0, st>>>(a);
+    TR_CHECK_LAUNCH();
+    k_tol_finalize<<<1, 256, 0, st>>>(p->partials, (int)blocks, p->tol_dev);
+    TR_CHECK_LAUNCH();
+    TR_CUDA(cudaMemcpyAsync(p->tol_host, p->tol_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    return TR_OK;
+}
+
+static double tolerance_from(const tr_pdhg_params* q, double num, double den) {
+    if (q->algorithm == TR_ALG_TVMW) {
+        if (std::isfinite(num) && std::isfinite(den))
+            return std::sqrt(std::max(num, 0.0)) / std::max(std::sqrt(std::max(den, 0.0)), 1e-12);
+        return INFINITY;
+    }
+    if (std::isfinite(num) && std::isfinite(den) && den > 0.0) return std::sqrt(std::max(num, 0.0)) / std::sqrt(den);
+    return INFINITY;
+}
+
+static bool same_config(const PdhgGraph* g, const tr_pdhg_state* s, const tr_pdhg_params* q, cudaStream_t st) {
+    return g && g->exec && g->stream == st && memcmp(&g->state, s, sizeof(*s)) == 0 &&
+           memcmp(&g->params, q, sizeof(*q)) == 0;
+}
+
+static tr_status run_impl(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_params* q, int max_iters, double tol,
+                          double* hist, int* done, cudaStream_t st) {
+    TR_TRY(validate(p, s, q));
+    int it = 0;
+    for (; it < max_iters; ++it) {
+        const bool use_graph = q->use_graph && it > 0;  // iteration 0 runs eagerly (allocates workspaces)
+        if (use_graph) {
+            if (!same_config(p->graph, s, q, st)) {
+                pdhg_destroy(p);
+                p->graph = new PdhgGraph();
+                p->graph->state = *s;
+                p->graph->params = *q;
+                p->graph->stream = st;
+                TR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                tr_status e = enqueue_iteration(p, s, q, st);
+                cudaGraph_t graph = nullptr;
+                cudaError_t ce = cudaStreamEndCapture(st, &graph);
+                if (e != TR_OK) {
+                    if (graph) cudaGraphDestroy(graph);
+                    pdhg_destroy(p);
+                    return e;
+                }
+                if (ce != cudaSuccess) {
+                    pdhg_destroy(p);
+                    return cuda_fail(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+                }
+                p->graph->graph = graph;
+                TR_CUDA(cudaGraphInstantiate(&p->graph->exec, graph, 0));
+            }
+            TR_CUDA(cudaGraphLaunch(p->graph->exec, st));
+        } else {
+            TR_TRY(enqueue_iteration(p, s, q, st));
+        }
+        TR_CUDA(cudaStreamSynchronize(st));
+        const double t = tolerance_from(q, p->tol_host[0], p->tol_host[1]);
+        if (hist) hist[it] = t;
+        if (!std::isfinite(p->tol_host[0]) || !std::isfinite(p->tol_host[1])) {
+            if (done) *done = it + 1;
+            return fail(TR_ERR_NONFINITE, "non-finite value in the tolerance reduction at iteration " +
+                                              std::to_string(it));
+        }
+        if (t < tol) {
+            ++it;
+            break;
+        }
+    }
+    if (done) *done = it;
+    return TR_OK;
+}
+
+}  // namespace tr
+
+using namespace tr;
+
+extern "C" tr_status tr_pdhg_run(tr_plan* plan, const tr_pdhg_state* state, const tr_pdhg_params* params,
+                                 int32_t max_iters, double tol, double* tol_history, int32_t* iters_done,
+                                 void* stream) {
+    if (!plan) return fail(TR_ERR_INVALID_ARG, "null plan");
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != plan->device) cudaSetDevice(plan->device);
+    int done = 0;
+    tr_status s = run_impl(plan, state, params, max_iters, tol, tol_history, &done, (cudaStream_t)stream);
+    if (iters_done) *iters_done = done;
+    if (prev >= 0 && prev != plan->device) cudaSetDevice(prev);
+    return s;
+}
+
+// ------------------------------------------------------------------ FP64 diagnostics
+__global__ void k_norm2(const float2* __restrict__ x, int64_t n, double* partials) {
+    double s = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float2 v = x[i];
+        s += (double)v.x * v.x + (double)v.y * v.y;
+    }
+    block_reduce_partials(s, 0.0, partials);
+}
+
+__global__ void k_scale(float2* x, int64_t n, const double* nrm2) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double inv = nrm2[0] > 0.0 ? 1.0 / sqrt(nrm2[0]) : 0.0;
+    x[i] = make_float2((float)(x[i].x * inv), (float)(x[i].y * inv));
+}
+
+// Power iteration on A^H W A with A = [F_b S_c] over all bins and echoes and W
+// the density weights (the operator the PDHG data term sees).  work_images is
+// caller scratch of (B, E, Z, Y, X) complex64; a k-space scratch is allocated.
+extern "C" tr_status tr_power_iteration(tr_plan* p, int32_t n_iter, void* work_images, double* norm_out,
+                                        void* stream) {
+    if (!p || !work_images || !norm_out || n_iter < 1) return fail(TR_ERR_INVALID_ARG, "tr_power_iteration: bad argument");
+    if (!p->maps) return fail(TR_ERR_INVALID_ARG, "coil maps not set (tr_plan_set_maps)");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t N = (int64_t)p->n[0] * p->n[1] * p->n[2];
+    const int64_t EN = (int64_t)p->E * N;
+    const int64_t tot = (int64_t)p->B * EN;
+    const int ncol = p->E * p->C;
+    float2* x = (float2*)work_images;
+    float2* ksp = nullptr;
+    double* part = nullptr;
+    double* d2 = nullptr;
+    TR_CUDA(cudaMalloc(&ksp, (size_t)std::max<int64_t>(p->total, 1) * ncol * sizeof(float2)));
+    const int nb = 1024;
+    TR_CUDA(cudaMalloc(&part, 2 * nb * sizeof(double)));
+    TR_CUDA(cudaMalloc(&d2, 2 * sizeof(double)));
+    tr_status rs = TR_OK;
+    double lam = 0.0;
+    for (int it = 0; it < n_iter && rs == TR_OK; ++it) {
+        k_norm2<<<nb, 256, 0, st>>>(x, tot, part);
+        k_tol_finalize<<<1, 256, 0, st>>>(part, nb, d2);
+        k_scale<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(x, tot, d2);
+        for (int b = 0; b < p->B && rs == TR_OK; ++b)
+            rs = nufft_forward_cols(p, b, x + b * EN, N, p->E, p->maps, p->C, kInterpStore, 0.f, nullptr,
+                                    ksp + p->bins[b].offset * ncol, st);
+        for (int b = 0; b < p->B && rs == TR_OK; ++b)
+            rs = nufft_adjoint_cols(p, b, ksp + p->bins[b].offset * ncol, p->E, p->maps, p->C, true, x + b * EN, N, st);
+        if (rs != TR_OK) break;
+        k_norm2<<<nb, 256, 0, st>>>(x, tot, part);
+        k_tol_finalize<<<1, 256, 0, st>>>(part, nb, d2);
+        double h[2];
+        cudaMemcpyAsync(h, d2, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
+            rs = fail(TR_ERR_CUDA, "power iteration failed");
+            break;
+        }
+        lam = std::sqrt(h[0]);  // ||A^H W A x|| with ||x|| = 1
+    }
+    cudaFree(ksp);
+    cudaFree(part);
+    cudaFree(d2);
+    if (rs == TR_OK) *norm_out = std::sqrt(lam);
+    return rs;
+}

@@ -1,0 +1,131 @@
+"""GPU parity of the b200 NUFFT against the CPU oracle (SigPy 0.1.27 restatement)."""
+
+import numpy as np
+import pytest
+
+from _fixtures import pkg
+from oracle import nufft as onf
+
+pytestmark = pytest.mark.gpu
+
+TOL_NUFFT = 1e-4   # north-star bar vs the reference NUFFT (relative L2)
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _coords(shape, M, rng, edge=True):
+    k = np.stack([rng.uniform(-n / 2, n / 2, M) for n in shape], -1).astype(np.float32)
+    k[0] = 0.0                       # the cone centre: five taps per axis
+    if edge:
+        k[1] = [-shape[0] / 2, -shape[1] / 2, -shape[2] / 2]   # the lowest grid edge (wraps)
+        k[2] = [shape[0] / 2 - 1e-3, 0.5, -0.25]
+        k[3] = [1.0, -2.0, 3.0]      # integer coordinates
+    return k
+
+
+SHAPES = [(12, 16, 20), (16, 20, 24), (28, 24, 20), (20, 32, 36), (48, 40, 12)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_single_image_forward_adjoint_match_oracle(shape):
+    torch = _torch()
+    nb = pkg("nufft_backend")
+    rng = np.random.default_rng(sum(shape))
+    M = 3000
+    k = _coords(shape, M, rng)
+    x = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    be = nb.B200NufftBackend(shape, [k[: M // 2], k[M // 2:]], 0)
+    for b, kb in enumerate([k[: M // 2], k[M // 2:]]):
+        y = be.forward(x, b)                      # numpy in -> numpy out
+        assert isinstance(y, np.ndarray) and y.shape == (kb.shape[0],)
+        yo = onf.nufft(x, kb)
+        assert onf.rel_l2(y, yo) < TOL_NUFFT
+        v = (rng.standard_normal(kb.shape[0]) + 1j * rng.standard_normal(kb.shape[0])).astype(np.complex64)
+        xa = be.adjoint(v, b)
+        xo = onf.nufft_adjoint(v, kb, shape)
+        assert xa.shape == shape
+        assert onf.rel_l2(xa, xo) < TOL_NUFFT
+    be.close()
+
+
+def test_forward_against_fp64_direct_nudft():
+    torch = _torch()
+    nb = pkg("nufft_backend")
+    rng = np.random.default_rng(7)
+    shape = (20, 24, 16)
+    k = _coords(shape, 800, rng, edge=False)
+    x = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    be = nb.B200NufftBackend(shape, [k], 0)
+    err = onf.rel_l2(be.forward(x, 0), onf.nudft(x, k))
+    # KB width 4 at 1.25x oversampling: ~1e-2 intrinsic error, same as the reference's SigPy defaults
+    assert err < 1.5e-2
+    be.close()
+
+
+def test_torch_in_torch_out_and_adjointness():
+    torch = _torch()
+    nb = pkg("nufft_backend")
+    rng = np.random.default_rng(3)
+    shape = (16, 16, 20)
+    k = _coords(shape, 2000, rng)
+    be = nb.B200NufftBackend(shape, [k], "cuda:0")
+    x = torch.randn(shape, dtype=torch.complex64, device="cuda")
+    y = torch.randn(2000, dtype=torch.complex64, device="cuda")
+    Ax = be.forward(x, 0)
+    Ahy = be.adjoint(y, 0)
+    assert isinstance(Ax, torch.Tensor) and Ax.is_cuda
+    lhs = torch.vdot(Ax.flatten(), y).item()
+    rhs = torch.vdot(x.flatten(), Ahy.flatten()).item()
+    assert abs(lhs - rhs) < 1e-4 * abs(lhs)
+    with pytest.raises(IndexError):
+        be.forward(x, 1)
+    be.close()
+
+
+def test_adjoint_is_bitwise_deterministic():
+    torch = _torch()
+    nb = pkg("nufft_backend")
+    rng = np.random.default_rng(5)
+    shape = (24, 20, 16)
+    # dense centre: many samples share tiles (the atomics-free gather must not depend on timing)
+    k = (rng.standard_normal((20000, 3)) * 1.5).astype(np.float32)
+    be = nb.B200NufftBackend(shape, [k], 0)
+    v = torch.randn(20000, dtype=torch.complex64, device="cuda")
+    a = be.adjoint(v, 0)
+    for _ in range(3):
+        b = be.adjoint(v, 0)
+        assert torch.equal(a, b)
+    xo = onf.nufft_adjoint(v.cpu().numpy(), k, shape)
+    assert onf.rel_l2(a.cpu().numpy(), xo) < TOL_NUFFT
+    be.close()
+
+
+@pytest.mark.parametrize("E,C", [(1, 1), (2, 3), (3, 16), (6, 16)])
+def test_batched_coil_echo_path(E, C):
+    torch = _torch()
+    nb = pkg("nufft_backend")
+    rng = np.random.default_rng(E * 31 + C)
+    shape = (12, 16, 20)
+    kb = [_coords(shape, 700, rng), _coords(shape, 400, rng)]
+    dcf = [rng.uniform(0.1, 1.0, 700).astype(np.float32), rng.uniform(0.1, 1.0, 400).astype(np.float32)]
+    mps = (rng.standard_normal((C,) + shape) + 1j * rng.standard_normal((C,) + shape)).astype(np.complex64)
+    img = (rng.standard_normal((E,) + shape) + 1j * rng.standard_normal((E,) + shape)).astype(np.complex64)
+    be = nb.B200NufftBackend(shape, kb, 0, dcf=dcf, n_coils=C, n_echoes=E)
+    be.set_maps(mps)
+    for b in range(2):
+        M = kb[b].shape[0]
+        ks = be.forward_bin(torch.from_numpy(img).cuda(), b)           # (M, E*C) sorted
+        ext = be.unsort_kspace(ks, b).cpu().numpy().reshape(E, C, M)
+        ref = onf.nufft(img[:, None] * mps[None], kb[b])              # (E, C, M)
+        assert onf.rel_l2(ext, ref) < TOL_NUFFT
+        q = (rng.standard_normal((E, C, M)) + 1j * rng.standard_normal((E, C, M))).astype(np.complex64)
+        qs = be.sort_kspace(torch.from_numpy(q.reshape(E * C, M)).cuda(), b)
+        g = be.adjoint_bin(qs, b, use_dcf=True).cpu().numpy()
+        gref = np.sum(onf.nufft_adjoint(dcf[b] * q, kb[b], shape) * np.conj(mps)[None], axis=1)
+        assert onf.rel_l2(g, gref) < TOL_NUFFT
+    be.close()
