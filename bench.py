@@ -1,0 +1,412 @@
+#!/usr/bin/env python3
+"""Benchmark of the b200 PDHG backend (toporecon TVME / TVM / TVMW).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config tvme-256] [--impl b200|reference]
+
+Workload (default ``tvme-256``): TVME at 256 x 256 x 128, 16 coils, 6 echoes,
+6 motion bins, 4096 cones x 800 readout points, lambda 1e-5, tol 1e-3, max 300
+iterations, seeded synthetic phantom (the reference's liver dataset is not
+available).  A "step" is one PDHG iteration over the whole batch (every bin,
+echo and coil).  W warm-up steps, then K steps timed with CUDA events on the
+solver's stream; then a full plain (zero-start) solve to tolerance and, when a
+trained network is present, a warm-started solve, each timed with CUDA events.
+
+The JSON line's ``value`` is the time-to-tolerance in seconds (warm-started
+when available, else plain); inputs are resident in HBM when timing starts.
+``e2e`` is the same solve through the public API from pinned host buffers
+(plan creation, H2D of k-space and maps, sort, solve, D2H of the image).
+``roofline`` reports the dominant NUFFT kernel (CUDA-event time of one launch
+on the full workload) against the measured HBM copy bandwidth.
+``cpu_baseline`` times the CPU oracle port (C/OpenMP KB loops + scipy.fft) on
+a bounded sample (one bin-echo-coil forward + adjoint NUFFT at full size plus
+one PDHG elementwise slice) scaled to the solve.
+
+Multi-GPU (torchrun): replicas only -- each rank solves its own copy of the
+problem (the single-device path does not shard); times are the max over ranks.
+Inputs exceed L2 (126 MB): every k-space column block and grid is larger.
+"""
+
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from dataclasses import replace
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+if str(REPO) not in sys.path:
+    sys.path.insert(0, str(REPO))
+PKG = "multinodemri-miccai26_b200"
+METRIC = "TVME time-to-tol 1e-3 (s) on 1 B200, warm-start vs plain PDHG; NUFFT GB/s"
+FALLBACK_HBM_GBS = 6650.0
+
+# Iterations to --tol of plain PDHG on each seeded workload, measured with the
+# b200 arm on the same seeded problem; the CPU reference arm cannot run a full
+# solve within minutes and extrapolates its per-iteration time with these.
+ITERS_TO_TOL = {"tvme-256": None, "tvme-256-dirichlet": None, "tvme-128": None, "tvmw-160": None, "tvm-64": 100}
+
+
+def parse(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[1])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--config", default="tvme-256")
+    ap.add_argument("--scale", type=float, default=1.0, help="shrink the workload (debug runs only)")
+    ap.add_argument("--max-iter", type=int, default=None)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true")
+    return ap.parse_args(argv)
+
+
+def log(*a):
+    print("[bench]", *a, file=sys.stderr, flush=True)
+
+
+def get_config(args):
+    syn = importlib.import_module(f"{PKG}.synthetic")
+    cfg = syn.CONFIGS[args.config]
+    if args.scale != 1.0:
+        cfg = syn.scaled(cfg, args.scale)
+    if args.max_iter:
+        cfg = replace(cfg, max_iter=args.max_iter)
+    return cfg
+
+
+def peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "of measured"
+    return FALLBACK_HBM_GBS, "of fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return float("nan")
+        sm = [num(r[1]) for r in rows]
+        pw = [num(r[3]) for r in rows]
+        smax = max(num(r[2]) for r in rows)
+        load = [s for s, p in zip(sm, pw) if p > 250] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": smax, "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int, device) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# --------------------------------------------------------------------------- CPU baseline
+def cpu_sample(cfg, ds_coord_bins, n_pairs: int = 1):
+    """Time the oracle port on a bounded sample: n_pairs full-size (b, e, c)
+    forward + adjoint NUFFTs and one elementwise TVME slice; returns seconds
+    per PDHG iteration extrapolated to the whole batch, and the threads used."""
+    from oracle import cgrid
+    cgrid.build()
+    rng = np.random.default_rng(123)
+    shape = tuple(cfg.img_shape)
+    k = ds_coord_bins[0].reshape(-1, 3)
+    x = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    t0 = time.perf_counter()
+    for _ in range(n_pairs):
+        y = cgrid.nufft(x, k)
+        cgrid.nufft_adjoint(y, k, shape)
+    t_pair = (time.perf_counter() - t0) / n_pairs
+    # elementwise: the oracle's TVME dual + primal on one (bin, echo-pair) slice
+    from oracle import pdhg as op
+    sl = (1, min(2, cfg.n_echoes)) + shape
+    u = (rng.standard_normal(sl) + 1j * rng.standard_normal(sl)).astype(np.complex64)
+    t0 = time.perf_counter()
+    d = op.dxf(u) + op.dyf(u) + op.dzf(u)
+    pm = u / np.maximum(1.0, np.abs(u) / 1e-5)
+    dv = op.dxb(d) + op.dyb(d) + op.dzb(d)
+    u2 = u - (1 / 6) * (dv + pm)
+    _ = 2 * u2 - u
+    t_elem = (time.perf_counter() - t0) * (cfg.n_bins * cfg.n_echoes) / (sl[0] * sl[1])
+    per_iter = t_pair * cfg.n_bins * cfg.n_echoes * cfg.n_coils + t_elem
+    return per_iter, cgrid.threads(), t_pair, t_elem
+
+
+def bin_coords(ds):
+    return [ds.coord[ds.bin_indices(b)] for b in range(ds.cfg.n_bins)]
+
+
+# --------------------------------------------------------------------------- b200 arm
+def run_b200(args):
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    syn = importlib.import_module(f"{PKG}.synthetic")
+    solver_mod = importlib.import_module(f"{PKG}.solver")
+    cfg = get_config(args)
+    t0 = time.perf_counter()
+    ds = syn.make_geometry(cfg)
+    log(f"geometry {time.perf_counter() - t0:.1f}s")
+    t0 = time.perf_counter()
+    syn.simulate_kspace_b200(ds, local)
+    log(f"k-space simulated on the GPU in {time.perf_counter() - t0:.1f}s")
+    coords, dcfs, ksps = bin_coords(ds), ds.bin_dcf(), ds.bin_ksp()
+    lam = cfg.lam
+    t0 = time.perf_counter()
+    solver = solver_mod.PdhgSolver(cfg.algorithm, cfg.img_shape, coords, dcfs, ds.mps, ksps,
+                                   l2_coupling=cfg.l2_coupling, lam_m=lam, lam_e=lam, lam_w1=lam, lam_w2=lam,
+                                   use_graph=not args.no_graph, device=local)
+    log(f"solver set up in {time.perf_counter() - t0:.1f}s")
+    st = solver.stream
+    E, C, B = solver.E, solver.C, solver.B
+    ncol = E * C
+    launches_per_iter = B * (4 + math.ceil(ncol / 128) + 3) + 3
+    if cfg.algorithm == "tvmw":
+        launches_per_iter += 6 * max(1, solver.backend.wavelet_levels)
+
+    clocks = ClockSampler(local)
+    # ---- warm-up and K timed steps (one PDHG iteration each)
+    solver.reset()
+    solver.iterate(max(3, args.warmup), tol=0.0)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(st)
+    solver.iterate(args.steps, tol=0.0)
+    ev1.record(st)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    ms_step = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world, device)
+
+    # ---- plain solve to tolerance
+    r_plain = solver.run(max_iter=cfg.max_iter, tol=cfg.tol)
+    plain_img = r_plain.image.clone()
+    t_plain = max_over_ranks(r_plain.seconds, world, device)
+    log(f"plain: {r_plain.iterations} iterations, {t_plain:.3f}s")
+
+    # ---- warm-started solve (learned initial iterate), when a trained network exists
+    warm = None
+    try:
+        ws = importlib.import_module(f"{PKG}.warmstart")
+        warm = ws.warm_solve(solver, cfg, max_iter=cfg.max_iter, tol=cfg.tol)
+    except (ImportError, FileNotFoundError, AttributeError) as exc:
+        log(f"warm start unavailable: {exc}")
+    clk = clocks.stop()
+
+    # ---- per-stage profile of bin 0 (roofline)
+    prof = solver.backend.profile(0, reps=3)
+    hbm, peak_src = peaks()
+    dom_name = max(prof, key=lambda k: prof[k]["ms"])
+    dom = prof[dom_name]
+    nufft_ms = sum(v["ms"] for v in prof.values())
+    nufft_bytes = sum(v["bytes"] for v in prof.values())
+
+    # ---- FP64 oracle agreement and warm/plain agreement
+    rel_warm = None
+    if warm is not None:
+        a = warm.image.reshape(-1)
+        rel_warm = float(torch.linalg.vector_norm(a - plain_img.reshape(-1)) /
+                         torch.linalg.vector_norm(plain_img.reshape(-1)))
+
+    value = warm.seconds if warm is not None else t_plain
+    value = max_over_ranks(value, world, device)
+
+    # ---- e2e through the public API from pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        ksp_h = [pin(k) for k in ksps]
+        mps_h = pin(ds.mps)
+        h2d = sum(k.numel() * 8 for k in ksp_h) + mps_h.numel() * 8 + sum(c.size * 4 for c in coords) + \
+            sum(d.size * 4 for d in dcfs)
+        solver.close()
+        del solver
+        torch.cuda.empty_cache()
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s2 = solver_mod.PdhgSolver(cfg.algorithm, cfg.img_shape, coords, dcfs, mps_h, ksp_h,
+                                   l2_coupling=cfg.l2_coupling, lam_m=lam, lam_e=lam, lam_w1=lam, lam_w2=lam,
+                                   use_graph=not args.no_graph, device=local)
+        if warm is not None:
+            r2 = ws.warm_solve(s2, cfg, max_iter=cfg.max_iter, tol=cfg.tol)
+        else:
+            r2 = s2.run(max_iter=cfg.max_iter, tol=cfg.tol)
+        out_h = torch.empty(r2.image.shape, dtype=torch.complex64, pin_memory=True)
+        out_h.copy_(r2.image, non_blocking=True)
+        torch.cuda.synchronize()
+        t_e2e = max_over_ranks(time.perf_counter() - t0, world, device)
+        e2e = {"value": round(t_e2e, 4), "unit": "s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(out_h.numel() * 8)}
+        s2.close()
+
+    # ---- CPU baseline (rank 0, N=1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        per_iter, threads, t_pair, t_elem = cpu_sample(cfg, coords)
+        cpu = {"value": round(per_iter * r_plain.iterations, 2), "unit": "s", "cores": threads, "kind": "port",
+               "sample": f"one full-size bin-echo-coil forward+adjoint NUFFT ({t_pair:.2f}s) x {B * E * C} "
+                         f"+ elementwise slice ({t_elem:.2f}s/iter), times {r_plain.iterations} plain iterations"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": round(value, 4),
+            "unit": "s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": max(3, args.warmup),
+            "ms_per_step": round(ms_step, 3),
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "c64",
+            "data": "synthetic",
+            "config": {"workload": cfg.name, "algorithm": cfg.algorithm, "img_shape_zyx": list(cfg.img_shape),
+                       "coils": C, "echoes": E, "bins": B, "cones": cfg.n_interleaves, "readout": cfg.n_readout,
+                       "tol": cfg.tol, "max_iter": cfg.max_iter, "l2_flush": "inputs larger than L2",
+                       "parallelism": "replicas" if world > 1 else "single-gpu"},
+            "time_to_tol_plain_s": round(t_plain, 4),
+            "iterations_plain": r_plain.iterations,
+            "time_to_tol_warm_s": None if warm is None else round(warm.seconds, 4),
+            "iterations_warm": None if warm is None else warm.iterations,
+            "warm_speedup": None if warm is None else round(t_plain / warm.seconds, 3),
+            "rel_l2_warm_vs_plain": rel_warm,
+            "iterations_per_s": round(1000.0 / ms_step, 3),
+            "nufft_gbs": round(nufft_bytes / (nufft_ms * 1e6), 1),
+            "nufft_stages": {k: {"ms": round(v["ms"], 4), "gbs": round(v["gbs"], 1),
+                                 "frac": round(v["gbs"] / hbm, 3)} for k, v in prof.items()},
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(dom["gbs"], 1), "peak": hbm,
+                         "unit": "GB/s", "frac": round(dom["gbs"] / hbm, 3), "peak_source": peak_src,
+                         "traffic": None, "algorithmic_bytes": dom["bytes"]},
+            "clocks": clk,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "gpu_launches": launches_per_iter * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg = get_config(args)
+    syn = importlib.import_module(f"{PKG}.synthetic")
+    rng = np.random.default_rng(cfg.seed)
+    coord = syn.cones_trajectory(cfg.img_shape, cfg.n_interleaves, cfg.n_readout, rng)
+    nb = cfg.n_bins
+    per_bin = coord[: max(1, cfg.n_interleaves // nb)]
+    iters = ITERS_TO_TOL.get(cfg.name) or cfg.max_iter
+    samples = []
+    for i in range(max(0, args.warmup) + args.steps):
+        t0 = time.perf_counter()
+        per_iter, threads, t_pair, t_elem = cpu_sample(cfg, [per_bin])
+        if i >= args.warmup:
+            samples.append(per_iter)
+    per_iter = statistics.mean(samples)
+    value = per_iter * iters
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(per_iter * 1e3, 1), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": cfg.name, "algorithm": cfg.algorithm, "img_shape_zyx": list(cfg.img_shape),
+                   "coils": cfg.n_coils, "echoes": cfg.n_echoes, "bins": cfg.n_bins, "tol": cfg.tol},
+        "iterations": iters,
+        "cpu_baseline": {"value": round(value, 2), "unit": "s", "cores": threads, "kind": "port",
+                         "sample": f"per step: one full-size bin-echo-coil NUFFT forward+adjoint x "
+                                   f"{cfg.n_bins * cfg.n_echoes * cfg.n_coils} + elementwise slice; "
+                                   f"x {iters} iterations"},
+        "e2e": {"value": round(value, 2), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main(argv=None):
+    args = parse(argv)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -155,10 +155,19 @@ tr_status tr_pdhg_run(tr_plan* plan, const tr_pdhg_state* state, const tr_pdhg_p
                       int32_t max_iters, double tol, double* tol_history, int32_t* iters_done,
                       void* stream);
 
-/* Diagnostics in FP64: operator-norm estimate of A = F S (power iteration,
- * n_iter steps) and the data residual 0.5*sum w |A u - y|^2. */
+/* Diagnostics in FP64: operator-norm estimate sqrt(||A^H W A||) of the data
+ * term (A = [F_b S_c], W = density weights) by n_iter power-iteration steps
+ * on caller scratch work_images (B, E, Z, Y, X), which must hold a nonzero start.
+ * No counterpart in the reference (it fixes sigma = tau = 1/6, tvme.py:968). */
 tr_status tr_power_iteration(tr_plan* plan, int32_t n_iter, void* work_images, double* norm_out,
                              void* stream);
+
+/* Per-stage device time of the batched NUFFT of one bin (all E x C columns):
+ * ms[8] and the algorithmic bytes[8] of each stage, in the order
+ * forward x, y, z, interpolation(+dual prox), gridding, adjoint z, y, x.
+ * Each stage is run reps times after one warm-up; used for roofline reports.
+ * Replaces the reference's wall-clock timers (tvme.py:509, :561-567). */
+tr_status tr_profile_nufft(tr_plan* plan, int32_t bin, int32_t reps, double* ms, double* bytes, void* stream);
 
 #ifdef __cplusplus
 }

@@ -372,8 +372,10 @@ struct SpreadArgs {
 template <int CPT>
 __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    __shared__ int run_start[27];
-    __shared__ int run_pref[28];
+    __shared__ int run_start[64];
+    __shared__ int run_pref[65];
+    __shared__ int nlist[3];
+    __shared__ int tlist[3][4];
     __shared__ int warp_cnt[8];
     __shared__ int warp_off[9];
     const int K = a.K;
@@ -392,20 +394,42 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
     const int Tz = min(kTile, a.os0 - t0z), Ty = min(kTile, a.os1 - t0y), Tx = min(kTile, a.os2 - t0x);
 
     const int tid = threadIdx.x;
-    if (tid < 27) {
-        const int dz = tid / 9 - 1, dy = (tid / 3) % 3 - 1, dx = tid % 3 - 1;
-        const int nz = pmod(tz + dz, a.nt0), ny = pmod(ty + dy, a.nt1), nx = pmod(tx + dx, a.nt2);
-        const int id = (nz * a.nt1 + ny) * a.nt2 + nx;
+    // Home tiles that can reach this tile: per axis, the distinct tiles holding
+    // floor(k) in [t0 - 2, t0 + T + 1] (wrapped).  At most four per axis when
+    // the last tile of the axis is shorter than the kernel reach.
+    if (tid < 3) {
+        const int t0 = tid == 0 ? t0z : (tid == 1 ? t0y : t0x);
+        const int Tn = tid == 0 ? Tz : (tid == 1 ? Ty : Tx);
+        const int osn = tid == 0 ? a.os0 : (tid == 1 ? a.os1 : a.os2);
+        int n = 0, prev = -1;
+        for (int pos = t0 - 2; pos <= t0 + Tn + 1; ++pos) {
+            const int tt = pmod(pos, osn) / kTile;
+            if (tt != prev && n < 4) {
+                bool seen = false;
+                for (int i = 0; i < n; ++i) seen |= (tlist[tid][i] == tt);
+                if (!seen) tlist[tid][n++] = tt;
+            }
+            prev = tt;
+        }
+        nlist[tid] = n;
+    }
+    __syncthreads();
+    const int nruns = nlist[0] * nlist[1] * nlist[2];
+    if (tid < nruns) {
+        const int iz = tid / (nlist[1] * nlist[2]);
+        const int iy = (tid / nlist[2]) % nlist[1];
+        const int ix = tid % nlist[2];
+        const int id = (tlist[0][iz] * a.nt1 + tlist[1][iy]) * a.nt2 + tlist[2][ix];
         run_start[tid] = a.tile_start[id];
         run_pref[tid + 1] = a.tile_start[id + 1] - a.tile_start[id];
     }
     __syncthreads();
     if (tid == 0) {
         run_pref[0] = 0;
-        for (int r = 0; r < 27; ++r) run_pref[r + 1] += run_pref[r];
+        for (int r = 0; r < nruns; ++r) run_pref[r + 1] += run_pref[r];
     }
     __syncthreads();
-    const int total = run_pref[27];
+    const int total = run_pref[nruns];
 
     const int p = tid & 63;
     const int pz = p >> 4, py = (p >> 2) & 3, px = p & 3;
@@ -615,14 +639,10 @@ static tr_status launch_line(tr_plan* p, int axis, const float2* in, float2* out
 
 static int coils_per_cta(int C) { return C <= 32 ? C : 32; }
 
-tr_status nufft_forward_cols(tr_plan* p, int bin, const float2* images, int64_t img_stride, int n_img,
-                             const float2* maps, int C, int mode, float sigma, const float2* y, float2* out,
-                             cudaStream_t st) {
-    const int ncol = n_img * C;
-    TR_TRY(ensure_nufft_buffers(p, (size_t)ncol));
-    const int Z = p->n[0], Y = p->n[1], X = p->n[2];
-    const int OSZ = p->os[0], OSY = p->os[1], OSX = p->os[2];
-    // x pass
+// ---- stage launchers (shared by the hot path and the profiler) ----
+static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_stride, int n_img, const float2* maps,
+                             int C, cudaStream_t st) {
+    const int Z = p->n[0], Y = p->n[1], X = p->n[2], OSX = p->os[2];
     FwdXArgs fa;
     fa.img = images;
     fa.img_stride = img_stride;
@@ -644,20 +664,30 @@ tr_status nufft_forward_cols(tr_plan* p, int bin, const float2* images, int64_t 
     fa.tw = p->ax[2].twiddle;
     fa.S = stages_of(p->ax[2]);
     fa.out = p->bufA;
-    fa.ncol = ncol;
-    {
-        const int W = fa.rows * fa.cc;
-        const size_t smem = fft_smem_bytes(OSX, W);
-        TR_TRY(set_smem_limit((const void*)k_fwd_x, smem));
-        dim3 grid((unsigned)((Z * Y + fa.rows - 1) / fa.rows), (unsigned)n_img, (unsigned)((C + fa.cc - 1) / fa.cc));
-        k_fwd_x<<<grid, 256, smem, st>>>(fa);
-        TR_CHECK_LAUNCH();
-    }
-    // y pass: [Z][Y -> OSY][OSX * ncol]
-    TR_TRY(launch_line(p, 1, p->bufA, p->bufB, Z, (int64_t)OSX * ncol, Y, OSY, p->ax[1].pad, 0, false, st));
-    // z pass: [1][Z -> OSZ][OSY * OSX * ncol]
-    TR_TRY(launch_line(p, 0, p->bufB, p->bufA, 1, (int64_t)OSY * OSX * ncol, Z, OSZ, p->ax[0].pad, 0, false, st));
-    // interpolation
+    fa.ncol = n_img * C;
+    const int W = fa.rows * fa.cc;
+    const size_t smem = fft_smem_bytes(OSX, W);
+    TR_TRY(set_smem_limit((const void*)k_fwd_x, smem));
+    dim3 grid((unsigned)((Z * Y + fa.rows - 1) / fa.rows), (unsigned)n_img, (unsigned)((C + fa.cc - 1) / fa.cc));
+    k_fwd_x<<<grid, 256, smem, st>>>(fa);
+    TR_CHECK_LAUNCH();
+    return TR_OK;
+}
+
+// y pass: [Z][Y -> OSY][OSX * ncol]
+static tr_status stage_fwd_y(tr_plan* p, int ncol, cudaStream_t st) {
+    return launch_line(p, 1, p->bufA, p->bufB, p->n[0], (int64_t)p->os[2] * ncol, p->n[1], p->os[1], p->ax[1].pad, 0,
+                       false, st);
+}
+
+// z pass: [1][Z -> OSZ][OSY * OSX * ncol]
+static tr_status stage_fwd_z(tr_plan* p, int ncol, cudaStream_t st) {
+    return launch_line(p, 0, p->bufB, p->bufA, 1, (int64_t)p->os[1] * p->os[2] * ncol, p->n[0], p->os[0],
+                       p->ax[0].pad, 0, false, st);
+}
+
+static tr_status stage_interp(tr_plan* p, int bin, int ncol, int mode, float sigma, const float2* y, float2* out,
+                              cudaStream_t st) {
     const Bin& b = p->bins[bin];
     if (b.count == 0) return TR_OK;
     int G = 1;
@@ -666,9 +696,9 @@ tr_status nufft_forward_cols(tr_plan* p, int bin, const float2* images, int64_t 
     const int64_t threads = b.count * G;
     const unsigned blocks = (unsigned)((threads + 255) / 256);
     const float4* ks = p->ks + b.offset;
-#define TR_INTERP(CPLV)                                                                                      \
-    k_interp<CPLV><<<blocks, 256, 0, st>>>(p->bufA, ks, b.count, ncol, G, OSZ, OSY, OSX, p->beta, mode, sigma, y, \
-                                           out)
+#define TR_INTERP(CPLV)                                                                                        \
+    k_interp<CPLV><<<blocks, 256, 0, st>>>(p->bufA, ks, b.count, ncol, G, p->os[0], p->os[1], p->os[2], p->beta, \
+                                           mode, sigma, y, out)
     if (cpl <= 1) TR_INTERP(1);
     else if (cpl <= 2) TR_INTERP(2);
     else if (cpl <= 3) TR_INTERP(3);
@@ -691,14 +721,9 @@ static tr_status launch_spread_t(const SpreadArgs& sa, unsigned ntiles, cudaStre
     return TR_OK;
 }
 
-tr_status nufft_adjoint_cols(tr_plan* p, int bin, const float2* ksp, int n_img, const float2* maps, int C,
-                             bool use_dcf, float2* images, int64_t img_stride, cudaStream_t st) {
-    const int ncol = n_img * C;
-    TR_TRY(ensure_nufft_buffers(p, (size_t)ncol));
-    const int Z = p->n[0], Y = p->n[1], X = p->n[2];
-    const int OSZ = p->os[0], OSY = p->os[1], OSX = p->os[2];
+// gridding, in column chunks of at most 128
+static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, bool use_dcf, cudaStream_t st) {
     const Bin& b = p->bins[bin];
-    // gridding, in column chunks of at most 128
     for (int col0 = 0; col0 < ncol; col0 += 128) {
         SpreadArgs sa;
         sa.ks = p->ks + b.offset;
@@ -710,9 +735,9 @@ tr_status nufft_adjoint_cols(tr_plan* p, int bin, const float2* ksp, int n_img, 
         sa.ncc = std::min(128, ncol - col0);
         sa.use_dcf = (use_dcf && p->has_dcf) ? 1 : 0;
         sa.grid = p->bufA;
-        sa.os0 = OSZ;
-        sa.os1 = OSY;
-        sa.os2 = OSX;
+        sa.os0 = p->os[0];
+        sa.os1 = p->os[1];
+        sa.os2 = p->os[2];
         sa.nt0 = p->ntile[0];
         sa.nt1 = p->ntile[1];
         sa.nt2 = p->ntile[2];
@@ -727,14 +752,28 @@ tr_status nufft_adjoint_cols(tr_plan* p, int bin, const float2* ksp, int n_img, 
         else if (cpt <= 24) TR_TRY(launch_spread_t<24>(sa, nt, st));
         else TR_TRY(launch_spread_t<32>(sa, nt, st));
     }
-    // z pass (inverse, crop to Z): [1][OSZ -> Z][OSY * OSX * ncol]
-    TR_TRY(launch_line(p, 0, p->bufA, p->bufB, 1, (int64_t)OSY * OSX * ncol, OSZ, Z, 0, p->ax[0].pad, true, st));
-    // y pass (inverse, crop to Y): [Z][OSY -> Y][OSX * ncol]
-    TR_TRY(launch_line(p, 1, p->bufB, p->bufA, Z, (int64_t)OSX * ncol, OSY, Y, 0, p->ax[1].pad, true, st));
-    // x pass with coil combine
+    return TR_OK;
+}
+
+// z pass (inverse, crop to Z): [1][OSZ -> Z][OSY * OSX * ncol]
+static tr_status stage_adj_z(tr_plan* p, int ncol, cudaStream_t st) {
+    return launch_line(p, 0, p->bufA, p->bufB, 1, (int64_t)p->os[1] * p->os[2] * ncol, p->os[0], p->n[0], 0,
+                       p->ax[0].pad, true, st);
+}
+
+// y pass (inverse, crop to Y): [Z][OSY -> Y][OSX * ncol]
+static tr_status stage_adj_y(tr_plan* p, int ncol, cudaStream_t st) {
+    return launch_line(p, 1, p->bufB, p->bufA, p->n[0], (int64_t)p->os[2] * ncol, p->os[1], p->n[1], 0,
+                       p->ax[1].pad, true, st);
+}
+
+// x pass with crop, apodisation and the coil combine
+static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, float2* images, int64_t img_stride,
+                             cudaStream_t st) {
+    const int Z = p->n[0], Y = p->n[1], X = p->n[2], OSX = p->os[2];
     AdjXArgs aa;
     aa.in = p->bufA;
-    aa.ncol = ncol;
+    aa.ncol = n_img * C;
     aa.maps = maps;
     aa.C = C;
     aa.cc = coils_per_cta(C);
@@ -761,6 +800,92 @@ tr_status nufft_adjoint_cols(tr_plan* p, int bin, const float2* ksp, int n_img, 
     k_adj_x<<<grid, 256, smem, st>>>(aa);
     TR_CHECK_LAUNCH();
     return TR_OK;
+}
+
+tr_status nufft_forward_cols(tr_plan* p, int bin, const float2* images, int64_t img_stride, int n_img,
+                             const float2* maps, int C, int mode, float sigma, const float2* y, float2* out,
+                             cudaStream_t st) {
+    const int ncol = n_img * C;
+    TR_TRY(ensure_nufft_buffers(p, (size_t)ncol));
+    TR_TRY(stage_fwd_x(p, images, img_stride, n_img, maps, C, st));
+    TR_TRY(stage_fwd_y(p, ncol, st));
+    TR_TRY(stage_fwd_z(p, ncol, st));
+    return stage_interp(p, bin, ncol, mode, sigma, y, out, st);
+}
+
+tr_status nufft_adjoint_cols(tr_plan* p, int bin, const float2* ksp, int n_img, const float2* maps, int C,
+                             bool use_dcf, float2* images, int64_t img_stride, cudaStream_t st) {
+    const int ncol = n_img * C;
+    TR_TRY(ensure_nufft_buffers(p, (size_t)ncol));
+    TR_TRY(stage_spread(p, bin, ksp, ncol, use_dcf, st));
+    TR_TRY(stage_adj_z(p, ncol, st));
+    TR_TRY(stage_adj_y(p, ncol, st));
+    return stage_adj_x(p, n_img, maps, C, images, img_stride, st);
+}
+
+// Per-stage CUDA-event timing of the batched NUFFT of one bin (all E echoes x
+// C coils), with the algorithmic bytes each stage must move.
+tr_status profile_nufft(tr_plan* p, int bin, int reps, double* ms, double* bytes, cudaStream_t st) {
+    const int E = p->E, C = p->C, ncol = E * C;
+    const int64_t N = (int64_t)p->n[0] * p->n[1] * p->n[2];
+    const int64_t G = (int64_t)p->os[0] * p->os[1] * p->os[2];
+    const int64_t XP = (int64_t)p->n[0] * p->n[1] * p->os[2];      // x-pass rows x OSX
+    const int64_t YP = (int64_t)p->n[0] * p->os[1] * p->os[2];      // y-pass output
+    const int64_t M = p->bins[bin].count;
+    const double c8 = 8.0;
+    if (!p->maps) return fail(TR_ERR_INVALID_ARG, "coil maps not set (tr_plan_set_maps)");
+    TR_TRY(ensure_nufft_buffers(p, (size_t)ncol));
+    float2 *img = nullptr, *ksp = nullptr, *yk = nullptr;
+    TR_CUDA(cudaMalloc(&img, (size_t)E * N * sizeof(float2)));
+    TR_CUDA(cudaMalloc(&ksp, (size_t)std::max<int64_t>(M, 1) * ncol * sizeof(float2)));
+    TR_CUDA(cudaMalloc(&yk, (size_t)std::max<int64_t>(M, 1) * ncol * sizeof(float2)));
+    cudaMemsetAsync(img, 0, (size_t)E * N * sizeof(float2), st);
+    cudaMemsetAsync(ksp, 0, (size_t)std::max<int64_t>(M, 1) * ncol * sizeof(float2), st);
+    cudaMemsetAsync(yk, 0, (size_t)std::max<int64_t>(M, 1) * ncol * sizeof(float2), st);
+    bytes[0] = c8 * (E * N + C * N + XP * ncol);
+    bytes[1] = c8 * ncol * (XP + YP);
+    bytes[2] = c8 * ncol * (YP + G);
+    bytes[3] = c8 * (G * ncol + 3 * M * ncol) + 16.0 * M;
+    bytes[4] = c8 * (M * ncol + G * ncol) + 16.0 * M;
+    bytes[5] = c8 * ncol * (G + YP);
+    bytes[6] = c8 * ncol * (YP + XP);
+    bytes[7] = c8 * (XP * ncol + C * N + E * N);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    tr_status rs = TR_OK;
+    for (int s = 0; s < 8 && rs == TR_OK; ++s) {
+        auto run = [&]() -> tr_status {
+            switch (s) {
+                case 0: return stage_fwd_x(p, img, N, E, p->maps, C, st);
+                case 1: return stage_fwd_y(p, ncol, st);
+                case 2: return stage_fwd_z(p, ncol, st);
+                case 3: return stage_interp(p, bin, ncol, kInterpDualProx, 1.f / 6.f, yk, ksp, st);
+                case 4: return stage_spread(p, bin, ksp, ncol, true, st);
+                case 5: return stage_adj_z(p, ncol, st);
+                case 6: return stage_adj_y(p, ncol, st);
+                default: return stage_adj_x(p, E, p->maps, C, img, N, st);
+            }
+        };
+        rs = run();  // warm-up
+        if (rs != TR_OK) break;
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < reps && rs == TR_OK; ++r) rs = run();
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rs = fail(TR_ERR_CUDA, "profiling failed");
+            break;
+        }
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        ms[s] = t / std::max(reps, 1);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(img);
+    cudaFree(ksp);
+    cudaFree(yk);
+    return rs;
 }
 
 static double apod_value(int i, int n, int L, int width, double beta) {
@@ -1101,6 +1226,13 @@ tr_status tr_nufft_forward_bin(tr_plan* p, int32_t bin, const void* images, void
     const int64_t N = (int64_t)p->n[0] * p->n[1] * p->n[2];
     return nufft_forward_cols(p, bin, (const float2*)images, N, p->E, p->maps, p->C, kInterpStore, 0.f, nullptr,
                               (float2*)ksp_internal, (cudaStream_t)stream);
+}
+
+tr_status tr_profile_nufft(tr_plan* p, int32_t bin, int32_t reps, double* ms, double* bytes, void* stream) {
+    TR_TRY(tr_plan_bin_offset(p, bin, nullptr, nullptr));
+    if (!ms || !bytes || reps < 1) return fail(TR_ERR_INVALID_ARG, "tr_profile_nufft: bad argument");
+    DeviceGuard g(p->device);
+    return profile_nufft(p, bin, reps, ms, bytes, (cudaStream_t)stream);
 }
 
 tr_status tr_nufft_adjoint_bin(tr_plan* p, int32_t bin, const void* ksp_internal, int32_t use_dcf, void* images,

@@ -118,14 +118,18 @@ class SigPyNufftBackend(NufftBackend):
 def _device_index(device) -> int:
     if device is None:
         return 0
-    if hasattr(device, "id"):
-        device = device.id
-    if hasattr(device, "index") and not isinstance(device, int):
-        return 0 if device.index is None else int(device.index)
     if isinstance(device, str):
         import torch
         d = torch.device(device)
+        if d.type != "cuda":
+            raise ValueError("the b200 backend runs on a CUDA device; got " + device)
         return 0 if d.index is None else int(d.index)
+    if hasattr(device, "id"):           # sigpy.Device
+        device = device.id
+    if type(device).__module__.startswith("torch"):
+        if device.type != "cuda":
+            raise ValueError("the b200 backend runs on a CUDA device")
+        return 0 if device.index is None else int(device.index)
     dev = int(device)
     if dev < 0:
         raise ValueError("the b200 backend runs on a CUDA device; got the CPU device")
@@ -328,6 +332,18 @@ class B200NufftBackend(NufftBackend):
         _lib.check(self._lib.tr_nufft_adjoint_bin(self._plan, b, ctypes.c_void_p(k.data_ptr()), int(use_dcf),
                                                   ctypes.c_void_p(out.data_ptr()), self._stream()))
         return out
+
+    STAGES = ("fwd_x", "fwd_y", "fwd_z", "interp", "spread", "adj_z", "adj_y", "adj_x")
+
+    def profile(self, bin_index: int = 0, reps: int = 5) -> dict:
+        """CUDA-event time (ms) and algorithmic bytes of each NUFFT stage of one bin."""
+        b = self._validate_bin(bin_index)
+        ms = (ctypes.c_double * 8)()
+        by = (ctypes.c_double * 8)()
+        _lib.check(self._lib.tr_profile_nufft(self._plan, b, int(reps), ms, by, self._stream()), "profile")
+        self._torch.cuda.synchronize(self.device)
+        return {name: {"ms": ms[i], "bytes": by[i], "gbs": by[i] / (ms[i] * 1e6) if ms[i] > 0 else 0.0}
+                for i, name in enumerate(self.STAGES)}
 
     def close(self) -> None:
         if getattr(self, "_plan", None):
