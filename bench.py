@@ -341,6 +341,7 @@ def run_b200(args):
                        "parallelism": "replicas" if world > 1 else "single-gpu"},
             "time_to_tol_plain_s": round(t_plain, 4),
             "iterations_plain": r_plain.iterations,
+            "tol_trace_plain": [round(t, 6) for t in r_plain.tols[::max(1, len(r_plain.tols) // 12)]],
             "time_to_tol_warm_s": None if warm is None else round(warm.seconds, 4),
             "iterations_warm": None if warm is None else warm.iterations,
             "warm_speedup": None if warm is None else round(t_plain / warm.seconds, 3),

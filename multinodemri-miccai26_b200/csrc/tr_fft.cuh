@@ -16,6 +16,21 @@
 
 namespace tr {
 
+// ------------------------------------------------------------------ async copies
+// cp.async global -> shared; bytes < size zero-fills the rest (bytes may be 0).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int bytes) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int bytes) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n" ::);
+    asm volatile("cp.async.wait_group 0;\n" ::);
+}
+
 // -i * z
 __device__ __forceinline__ float2 mul_mi(float2 z) { return make_float2(z.y, -z.x); }
 // +i * z

@@ -113,37 +113,44 @@ struct FwdXArgs {
 __global__ void __launch_bounds__(256) k_fwd_x(FwdXArgs a) {
     extern __shared__ float2 sm[];
     const int W = a.rows * a.cc;
+    const int L = a.S.L;
     float2* smA = sm;
-    float2* smB = sm + a.S.L * W;
-    float2* tws = sm + 2 * a.S.L * W;
-    for (int i = threadIdx.x; i < a.S.L; i += blockDim.x) tws[i] = a.tw[i];
-    __syncthreads();
+    float2* smB = sm + L * W;
+    float2* tws = sm + 2 * L * W;
     const int row0 = blockIdx.x * a.rows;
     const int img = blockIdx.y;
     const int c0 = blockIdx.z * a.cc;
     const int nrows = a.Z * a.Y;
     const float2* __restrict__ src = a.img + (int64_t)img * a.img_stride;
-    auto load = [&](int m, int w) -> float2 {
+    for (int i = threadIdx.x; i < L; i += blockDim.x) tws[i] = a.tw[i];
+    // fill: smA[m][w] = image * map * apodisation * scale at padded, shifted position m
+    const int total = L * W;
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int m = idx / W, w = idx - m * W;
         const int rl = w / a.cc, cl = w - rl * a.cc;
-        const int row = row0 + rl;
-        const int c = c0 + cl;
+        const int row = row0 + rl, c = c0 + cl;
         int j = m + a.h;
-        if (j >= a.S.L) j -= a.S.L;
+        if (j >= L) j -= L;
         const int x = j - a.pad;
-        if (x < 0 || x >= a.X || row >= nrows || c >= a.C) return make_float2(0.f, 0.f);
-        const int z = row / a.Y, y = row - z * a.Y;
-        float2 v = src[(int64_t)row * a.X + x];
-        if (a.maps) v = cmul(v, a.maps[((int64_t)row * a.X + x) * a.C + c]);
-        const float s = a.apz[z] * a.apy[y] * a.apx[x] * a.scale;
-        return cscale(v, s);
-    };
+        float2 v = make_float2(0.f, 0.f);
+        if (x >= 0 && x < a.X && row < nrows && c < a.C) {
+            const int z = row / a.Y, y = row - z * a.Y;
+            v = src[(int64_t)row * a.X + x];
+            if (a.maps) v = cmul(v, a.maps[((int64_t)row * a.X + x) * a.C + c]);
+            v = cscale(v, a.apz[z] * a.apy[y] * a.apx[x] * a.scale);
+        }
+        smA[idx] = v;
+    }
+    __syncthreads();
+    auto load = [smA, W](int m, int w) -> float2 { return smA[m * W + w]; };
     auto store = [&](int k, int w, float2 v) {
         const int rl = w / a.cc, cl = w - rl * a.cc;
         const int row = row0 + rl;
         const int c = c0 + cl;
         if (row >= nrows || c >= a.C) return;
         int g = k + a.h;
-        if (g >= a.S.L) g -= a.S.L;
+        if (g >= L) g -= L;
         a.out[((int64_t)row * a.OSX + g) * a.ncol + (int64_t)img * a.C + c] = v;
     };
     fft_run(smA, smB, tws, a.S, W, false, load, store);
@@ -159,36 +166,66 @@ struct LineArgs {
     int64_t inner;
     int Lin, Lout, p_in, p_out, h;
     int W;
+    int vec16;              // rows are 16-byte aligned: copy two elements per cp.async
     bool inv;
     const float2* tw;
     FftStages S;
 };
 
+// The CTA's [L][W] tile is staged with cp.async (every load in flight at
+// once, zero-filled pad rows and tail columns), then all stages run from
+// shared memory and the last stage stores straight to global memory.
 __global__ void __launch_bounds__(256) k_line(LineArgs a) {
     extern __shared__ float2 sm[];
     const int W = a.W;
+    const int L = a.S.L;
     float2* smA = sm;
-    float2* smB = sm + a.S.L * W;
-    float2* tws = sm + 2 * a.S.L * W;
-    for (int i = threadIdx.x; i < a.S.L; i += blockDim.x) tws[i] = a.tw[i];
-    __syncthreads();
+    float2* smB = sm + L * W;
+    float2* tws = sm + 2 * L * W;
     const int64_t q0 = (int64_t)blockIdx.x * W;
     const int64_t outer = blockIdx.y;
     const float2* __restrict__ in = a.in + outer * a.Lin * a.inner;
     float2* __restrict__ out = a.out + outer * a.Lout * a.inner;
-    const int L = a.S.L;
-    auto load = [&](int m, int w) -> float2 {
-        const int64_t q = q0 + w;
-        int j = m + a.h;
-        if (j >= L) j -= L;
-        const int i = j - a.p_in;
-        if (q >= a.inner || i < 0 || i >= a.Lin) return make_float2(0.f, 0.f);
-        return in[(int64_t)i * a.inner + q];
-    };
+    for (int i = threadIdx.x; i < L; i += blockDim.x) tws[i] = a.tw[i];
+    if (a.vec16) {
+        const int nch = W >> 1;
+        for (int idx = threadIdx.x; idx < L * nch; idx += blockDim.x) {
+            const int m = idx / nch, ch = idx - m * nch;
+            int j = m + a.h;
+            if (j >= L) j -= L;
+            const int i = j - a.p_in;
+            const int64_t q = q0 + 2 * ch;
+            int bytes = 0;
+            const float2* g = a.in;
+            if (i >= 0 && i < a.Lin && q < a.inner) {
+                bytes = (q + 1 < a.inner) ? 16 : 8;
+                g = in + (int64_t)i * a.inner + q;
+            }
+            cp_async16(smA + m * W + 2 * ch, g, bytes);
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < L * W; idx += blockDim.x) {
+            const int m = idx / W, w = idx - m * W;
+            int j = m + a.h;
+            if (j >= L) j -= L;
+            const int i = j - a.p_in;
+            const int64_t q = q0 + w;
+            int bytes = 0;
+            const float2* g = a.in;
+            if (i >= 0 && i < a.Lin && q < a.inner) {
+                bytes = 8;
+                g = in + (int64_t)i * a.inner + q;
+            }
+            cp_async8(smA + idx, g, bytes);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    auto load = [smA, W](int m, int w) -> float2 { return smA[m * W + w]; };
     auto store = [&](int k, int w, float2 v) {
         const int64_t q = q0 + w;
         int o = k + a.h - a.p_out;
-        o = o % L;
+        o %= L;
         if (o < 0) o += L;
         if (q >= a.inner || o >= a.Lout) return;
         out[(int64_t)o * a.inner + q] = v;
@@ -227,21 +264,30 @@ __global__ void __launch_bounds__(256) k_adj_x(AdjXArgs a) {
     float2* acc = tws + L;                  // [rows][X]
     for (int i = threadIdx.x; i < L; i += blockDim.x) tws[i] = a.tw[i];
     for (int i = threadIdx.x; i < a.rows * a.X; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
-    __syncthreads();
     const int row0 = blockIdx.x * a.rows;
     const int img = blockIdx.y;
     const int nrows = a.Z * a.Y;
     // buffer free during the last stage (the other one is its source)
     float2* ep = (a.S.nstages == 1) ? buf1 : (((a.S.nstages - 1) % 2 == 0) ? buf1 : buf0);
     for (int c0 = 0; c0 < a.C; c0 += a.cc) {
-        auto load = [&](int m, int w) -> float2 {
+        // stage the [L][W] input tile (centred shift applied on the row index)
+        for (int idx = threadIdx.x; idx < L * W; idx += blockDim.x) {
+            const int m = idx / W, w = idx - m * W;
             const int rl = w / a.cc, cl = w - rl * a.cc;
             const int row = row0 + rl, c = c0 + cl;
-            if (row >= nrows || c >= a.C) return make_float2(0.f, 0.f);
             int j = m + a.h;
             if (j >= L) j -= L;
-            return a.in[((int64_t)row * a.OSX + j) * a.ncol + (int64_t)img * a.C + c];
-        };
+            int bytes = 0;
+            const float2* g = a.in;
+            if (row < nrows && c < a.C) {
+                bytes = 8;
+                g = a.in + ((int64_t)row * a.OSX + j) * a.ncol + (int64_t)img * a.C + c;
+            }
+            cp_async8(buf0 + idx, g, bytes);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        auto load = [buf0, W](int m, int w) -> float2 { return buf0[m * W + w]; };
         auto store = [&](int k, int w, float2 v) {
             int o = k + a.h - a.pad;
             o %= L;
@@ -307,7 +353,7 @@ __global__ void __launch_bounds__(256) k_interp(const float2* __restrict__ grid,
     for (int tz = 0; tz < 5; ++tz) {
         if (wz[tz] == 0.f) continue;
         const int64_t zoff = (int64_t)pmod(bz + tz, os0) * os1;
-#pragma unroll 1
+#pragma unroll
         for (int ty = 0; ty < 5; ++ty) {
             if (wy[ty] == 0.f) continue;
             const float wzy = wz[tz] * wy[ty];
@@ -360,7 +406,7 @@ struct SpreadArgs {
     const int32_t* tile_start; // bin base [ntiles + 1]
     const int32_t* tile_order; // bin base [ntiles] or null
     const float2* vals;        // (M_b, ncol) bin base
-    int ncol, col0, ncc;
+    int ncol, cchunk;          // columns per CTA (blockIdx.y selects the chunk)
     int use_dcf;
     float2* grid;              // (OSZ, OSY, OSX, ncol)
     int os0, os1, os2;
@@ -385,6 +431,8 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
     float* c_d = reinterpret_cast<float*>(c_s + K);              // [K]
     float2* dq = reinterpret_cast<float2*>(c_d + K);             // [max(K, 64)][ncc] (80 K bytes in: 8-aligned)
 
+    const int col0 = blockIdx.y * a.cchunk;
+    const int ncc = min(a.cchunk, a.ncol - col0);
     const int tile = a.tile_order ? a.tile_order[blockIdx.x] : (int)blockIdx.x;
     const int tz = tile / (a.nt1 * a.nt2);
     const int trem = tile - tz * a.nt1 * a.nt2;
@@ -430,6 +478,16 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
     }
     __syncthreads();
     const int total = run_pref[nruns];
+    if (total == 0) {   // empty neighbourhood: the tile is zero
+        for (int i = tid; i < kTilePts * ncc; i += blockDim.x) {
+            const int pp = i / ncc, col = i - pp * ncc;
+            const int qz = pp >> 4, qy = (pp >> 2) & 3, qx = pp & 3;
+            if (qz >= Tz || qy >= Ty || qx >= Tx) continue;
+            const int64_t g = ((int64_t)(t0z + qz) * a.os1 + (t0y + qy)) * a.os2 + (t0x + qx);
+            a.grid[g * a.ncol + col0 + col] = make_float2(0.f, 0.f);
+        }
+        return;
+    }
 
     const int p = tid & 63;
     const int pz = p >> 4, py = (p >> 2) & 3, px = p & 3;
@@ -492,9 +550,9 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
         }
         __syncthreads();
         // ---- phase 2: stage weighted values
-        for (int i = tid; i < nc * a.ncc; i += blockDim.x) {
-            const int cand = i / a.ncc, col = i - cand * a.ncc;
-            float2 v = a.vals[(int64_t)c_s[cand] * a.ncol + a.col0 + col];
+        for (int i = tid; i < nc * ncc; i += blockDim.x) {
+            const int cand = i / ncc, col = i - cand * ncc;
+            float2 v = a.vals[(int64_t)c_s[cand] * a.ncol + col0 + col];
             dq[i] = cscale(v, c_d[cand]);
         }
         __syncthreads();
@@ -506,11 +564,11 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
             if ((unsigned)az > 4u || (unsigned)ay > 4u || (unsigned)ax > 4u) continue;
             const float w = c_w[15 * cc + az] * c_w[15 * cc + 5 + ay] * c_w[15 * cc + 10 + ax];
             if (w == 0.f) continue;
-            const float2* row = dq + cc * a.ncc;
+            const float2* row = dq + cc * ncc;
 #pragma unroll
             for (int j = 0; j < CPT; ++j) {
                 const int col = cs + 4 * j;
-                if (col < a.ncc) {
+                if (col < ncc) {
                     const float2 v = row[col];
                     acc[j].x += w * v.x;
                     acc[j].y += w * v.y;
@@ -523,15 +581,15 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
         const int col = cs + 4 * j;
-        if (col < a.ncc) dq[p * a.ncc + col] = acc[j];
+        if (col < ncc) dq[p * ncc + col] = acc[j];
     }
     __syncthreads();
-    for (int i = tid; i < kTilePts * a.ncc; i += blockDim.x) {
-        const int pp = i / a.ncc, col = i - pp * a.ncc;
+    for (int i = tid; i < kTilePts * ncc; i += blockDim.x) {
+        const int pp = i / ncc, col = i - pp * ncc;
         const int qz = pp >> 4, qy = (pp >> 2) & 3, qx = pp & 3;
         if (qz >= Tz || qy >= Ty || qx >= Tx) continue;
         const int64_t g = ((int64_t)(t0z + qz) * a.os1 + (t0y + qy)) * a.os2 + (t0x + qx);
-        a.grid[g * a.ncol + a.col0 + col] = dq[i];
+        a.grid[g * a.ncol + col0 + col] = dq[i];
     }
 }
 
@@ -626,6 +684,7 @@ static tr_status launch_line(tr_plan* p, int axis, const float2* in, float2* out
     la.p_out = p_out;
     la.h = A.h;
     la.W = p->line_width;
+    la.vec16 = ((inner % 2) == 0 && (la.W % 2) == 0 && ((uintptr_t)in % 16) == 0) ? 1 : 0;
     la.inv = inv;
     la.tw = A.twiddle;
     la.S = stages_of(A);
@@ -711,48 +770,43 @@ static tr_status stage_interp(tr_plan* p, int bin, int ncol, int mode, float sig
 }
 
 template <int CPT>
-static tr_status launch_spread_t(const SpreadArgs& sa, unsigned ntiles, cudaStream_t st) {
+static tr_status launch_spread_t(const SpreadArgs& sa, unsigned ntiles, unsigned nchunks, cudaStream_t st) {
     const size_t cand_bytes = (size_t)sa.K * (3 * 4 + 15 * 4 + 4 + 4) + 8;
-    const size_t dq_bytes = (size_t)std::max(sa.K, kTilePts) * sa.ncc * sizeof(float2);
+    const size_t dq_bytes = (size_t)std::max(sa.K, kTilePts) * sa.cchunk * sizeof(float2);
     const size_t smem = cand_bytes + dq_bytes;
     TR_TRY(set_smem_limit((const void*)k_spread<CPT>, smem));
-    k_spread<CPT><<<ntiles, 256, smem, st>>>(sa);
+    k_spread<CPT><<<dim3(ntiles, nchunks), 256, smem, st>>>(sa);
     TR_CHECK_LAUNCH();
     return TR_OK;
 }
 
-// gridding, in column chunks of at most 128
+// gridding: one CTA per (4x4x4 tile, chunk of <= 32 columns)
 static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, bool use_dcf, cudaStream_t st) {
     const Bin& b = p->bins[bin];
-    for (int col0 = 0; col0 < ncol; col0 += 128) {
-        SpreadArgs sa;
-        sa.ks = p->ks + b.offset;
-        sa.tile_start = p->tile_start + (int64_t)bin * (p->ntiles + 1);
-        sa.tile_order = p->tile_order + (int64_t)bin * p->ntiles;
-        sa.vals = ksp;
-        sa.ncol = ncol;
-        sa.col0 = col0;
-        sa.ncc = std::min(128, ncol - col0);
-        sa.use_dcf = (use_dcf && p->has_dcf) ? 1 : 0;
-        sa.grid = p->bufA;
-        sa.os0 = p->os[0];
-        sa.os1 = p->os[1];
-        sa.os2 = p->os[2];
-        sa.nt0 = p->ntile[0];
-        sa.nt1 = p->ntile[1];
-        sa.nt2 = p->ntile[2];
-        sa.beta = p->beta;
-        sa.K = std::max(64, std::min(256, (int)((48 * 1024) / (sa.ncc * sizeof(float2)))));
-        const int cpt = (sa.ncc + 3) / 4;
-        const unsigned nt = (unsigned)p->ntiles;
-        if (cpt <= 1) TR_TRY(launch_spread_t<1>(sa, nt, st));
-        else if (cpt <= 4) TR_TRY(launch_spread_t<4>(sa, nt, st));
-        else if (cpt <= 8) TR_TRY(launch_spread_t<8>(sa, nt, st));
-        else if (cpt <= 16) TR_TRY(launch_spread_t<16>(sa, nt, st));
-        else if (cpt <= 24) TR_TRY(launch_spread_t<24>(sa, nt, st));
-        else TR_TRY(launch_spread_t<32>(sa, nt, st));
-    }
-    return TR_OK;
+    SpreadArgs sa;
+    sa.ks = p->ks + b.offset;
+    sa.tile_start = p->tile_start + (int64_t)bin * (p->ntiles + 1);
+    sa.tile_order = p->tile_order + (int64_t)bin * p->ntiles;
+    sa.vals = ksp;
+    sa.ncol = ncol;
+    sa.cchunk = std::min(32, ncol);
+    sa.use_dcf = (use_dcf && p->has_dcf) ? 1 : 0;
+    sa.grid = p->bufA;
+    sa.os0 = p->os[0];
+    sa.os1 = p->os[1];
+    sa.os2 = p->os[2];
+    sa.nt0 = p->ntile[0];
+    sa.nt1 = p->ntile[1];
+    sa.nt2 = p->ntile[2];
+    sa.beta = p->beta;
+    sa.K = 128;
+    const int cpt = (sa.cchunk + 3) / 4;
+    const unsigned nt = (unsigned)p->ntiles;
+    const unsigned nch = (unsigned)((ncol + sa.cchunk - 1) / sa.cchunk);
+    if (cpt <= 1) return launch_spread_t<1>(sa, nt, nch, st);
+    if (cpt <= 2) return launch_spread_t<2>(sa, nt, nch, st);
+    if (cpt <= 4) return launch_spread_t<4>(sa, nt, nch, st);
+    return launch_spread_t<8>(sa, nt, nch, st);
 }
 
 // z pass (inverse, crop to Z): [1][OSZ -> Z][OSY * OSX * ncol]
