@@ -1,0 +1,59 @@
+"""Per-stage timing of the b200 NUFFT on one bin (CUDA events), for roofline work.
+
+    python multinodemri-miccai26_b200/profile_nufft.py --shape 96 128 128 --coils 16 --echoes 2 --reps 3
+
+Builds one bin of the synthetic cones trajectory (``--cones`` interleaves of
+``--readout`` points), random coil maps, and runs ``B200NufftBackend.profile``:
+each of the eight batched-NUFFT stages (forward x / y / z passes,
+interpolation with the fused dual prox, gridding, adjoint z / y / x passes)
+once as warm-up and ``--reps`` times timed.  Prints one JSON line with ms,
+algorithmic bytes and GB/s per stage.  Small shapes keep ``ncu --set full``
+captures to a few GB of device memory.
+"""
+
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parents[1]
+if str(REPO) not in sys.path:
+    sys.path.insert(0, str(REPO))
+PKG = Path(__file__).resolve().parent.name
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--shape", type=int, nargs=3, default=[96, 128, 128])
+    ap.add_argument("--coils", type=int, default=16)
+    ap.add_argument("--echoes", type=int, default=2)
+    ap.add_argument("--cones", type=int, default=700)
+    ap.add_argument("--readout", type=int, default=600)
+    ap.add_argument("--reps", type=int, default=3)
+    args = ap.parse_args(argv)
+    import torch
+    syn = importlib.import_module(f"{PKG}.synthetic")
+    nb = importlib.import_module(f"{PKG}.nufft_backend")
+    shape = tuple(args.shape)
+    rng = np.random.default_rng(0)
+    coord = syn.cones_trajectory(shape, args.cones, args.readout, rng).reshape(-1, 3)
+    dcf = syn.density(coord, shape)
+    be = nb.B200NufftBackend(shape, [coord], 0, dcf=[dcf], n_coils=args.coils, n_echoes=args.echoes)
+    mps = syn.coil_maps(shape, args.coils, rng)
+    be.set_maps(mps)
+    prof = be.profile(0, reps=args.reps)
+    torch.cuda.synchronize()
+    out = {"shape_zyx": list(shape), "os_shape": list(be.os_shape), "coils": args.coils, "echoes": args.echoes,
+           "samples": int(coord.shape[0]), "stages": {k: {kk: round(vv, 4) for kk, vv in v.items()}
+                                                      for k, v in prof.items()}}
+    print(json.dumps(out))
+    be.close()
+
+
+if __name__ == "__main__":
+    main()
