@@ -206,6 +206,93 @@ __device__ __forceinline__ void fft_stage_dispatch(int R, const float2* tw, int 
     }
 }
 
+// ------------------------------------------------------------------ compile-time FFT
+// Same Stockham stages, with L, W, the thread count and every radix, butterfly
+// count, stride and twiddle step known at compile time (fully unrolled, no
+// runtime division).  The radix sequence matches factor_radices() on the host:
+// 7s, 5s, 3s first, then 8s, 4s, 2s.
+__host__ __device__ constexpr int ct_radix(int L, int s) {
+    int n = L, i = 0;
+    for (int r : {7, 5, 3}) {
+        while (n % r == 0) {
+            if (i == s) return r;
+            n /= r;
+            ++i;
+        }
+    }
+    for (int r : {8, 4, 2}) {
+        while (n % r == 0) {
+            if (i == s) return r;
+            n /= r;
+            ++i;
+        }
+    }
+    return 0;
+}
+__host__ __device__ constexpr int ct_nstages(int L) {
+    int s = 0;
+    while (ct_radix(L, s) != 0) ++s;
+    return s;
+}
+
+template <int L, int W, int NT, bool INV, int s, int Ns>
+struct CtStage {
+    template <class Store>
+    __device__ __forceinline__ static void run(const float2* __restrict__ src, float2* __restrict__ dst,
+                                               const float2* __restrict__ tw, Store& store) {
+        constexpr int S = ct_nstages(L);
+        constexpr int R = ct_radix(L, s);
+        constexpr int NB = L / R;
+        constexpr int TOTAL = NB * W;
+        constexpr int STEP = L / (Ns * R);
+        constexpr int ITERS = (TOTAL + NT - 1) / NT;
+#pragma unroll
+        for (int it = 0; it < ITERS; ++it) {
+            const int idx = (int)threadIdx.x + it * NT;
+            if (TOTAL % NT == 0 || idx < TOTAL) {
+                const int j = idx / W;
+                const int w = idx - j * W;
+                const int k = (Ns == 1) ? 0 : j % Ns;
+                float2 v[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    float2 x = src[(j + r * NB) * W + w];
+                    if (Ns > 1 && r > 0) {
+                        float2 t = tw[k * r * STEP];
+                        if (INV) t.y = -t.y;
+                        x = cmul(x, t);
+                    }
+                    v[r] = x;
+                }
+                Dft<R>::run(v, INV);
+                const int d0 = (Ns == 1) ? j * R : (j / Ns) * Ns * R + k;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (s == S - 1) store(d0 + r * Ns, w, v[r]);
+                    else dst[(d0 + r * Ns) * W + w] = v[r];
+                }
+            }
+        }
+        if constexpr (s < S - 1) {
+            __syncthreads();
+            CtStage<L, W, NT, INV, s + 1, Ns * R>::run(dst, const_cast<float2*>(src), tw, store);
+        }
+    }
+};
+
+// Transform the [L][W] tile in A (A is clobbered); the last stage hands every
+// output element to store(k, w, v).
+template <int L, int W, int NT, bool INV, class Store>
+__device__ __forceinline__ void fft_ct(float2* A, float2* B, const float2* tw, Store& store) {
+    CtStage<L, W, NT, INV, 0, 1>::run(A, B, tw, store);
+}
+
+// Buffer that the last stage of an L-point fft_ct does not read.
+template <int L>
+__device__ __forceinline__ float2* fft_ct_free(float2* A, float2* B) {
+    return ((ct_nstages(L) - 1) % 2 == 0) ? B : A;
+}
+
 // Full transform: load(m, w) -> input element m of column w; store(k, w, v)
 // receives output element k.  smA / smB are [L][W] scratch buffers.  The call
 // ends with a __syncthreads() only between stages; callers that read smem

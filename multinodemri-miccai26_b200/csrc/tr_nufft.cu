@@ -323,6 +323,181 @@ __global__ void __launch_bounds__(256) k_adj_x(AdjXArgs a) {
     }
 }
 
+// ------------------------------------------------------------------ compile-time variants
+// The same three FFT kernels with L and W fixed at compile time (fft_ct):
+// used for the transform lengths of the supported workloads.
+#define TR_CT_LENGTHS(X) X(60) X(80) X(100) X(120) X(140) X(160) X(200) X(240) X(320)
+
+template <int L, int W, bool INV>
+__global__ void __launch_bounds__(256) k_line_ct(LineArgs a) {
+    extern __shared__ float2 sm[];
+    float2* smA = sm;
+    float2* smB = sm + L * W;
+    float2* tws = sm + 2 * L * W;
+    const int64_t q0 = (int64_t)blockIdx.x * W;
+    const int64_t outer = blockIdx.y;
+    const float2* __restrict__ in = a.in + outer * a.Lin * a.inner;
+    float2* __restrict__ out = a.out + outer * a.Lout * a.inner;
+    for (int i = threadIdx.x; i < L; i += 256) tws[i] = a.tw[i];
+    if (a.vec16) {
+        constexpr int NCH = W / 2;
+#pragma unroll 4
+        for (int idx = threadIdx.x; idx < L * NCH; idx += 256) {
+            const int m = idx / NCH, ch = idx - m * NCH;
+            int j = m + a.h;
+            if (j >= L) j -= L;
+            const int i = j - a.p_in;
+            const int64_t q = q0 + 2 * ch;
+            int bytes = 0;
+            const float2* g = a.in;
+            if (i >= 0 && i < a.Lin && q < a.inner) {
+                bytes = (q + 1 < a.inner) ? 16 : 8;
+                g = in + (int64_t)i * a.inner + q;
+            }
+            cp_async16(smA + m * W + 2 * ch, g, bytes);
+        }
+    } else {
+#pragma unroll 4
+        for (int idx = threadIdx.x; idx < L * W; idx += 256) {
+            const int m = idx / W, w = idx - m * W;
+            int j = m + a.h;
+            if (j >= L) j -= L;
+            const int i = j - a.p_in;
+            const int64_t q = q0 + w;
+            int bytes = 0;
+            const float2* g = a.in;
+            if (i >= 0 && i < a.Lin && q < a.inner) {
+                bytes = 8;
+                g = in + (int64_t)i * a.inner + q;
+            }
+            cp_async8(smA + idx, g, bytes);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int shift = a.h - a.p_out;
+    const int Lout = a.Lout;
+    const int64_t inner = a.inner;
+    auto store = [&](int k, int w, float2 v) {
+        int o = k + shift;
+        o = o >= L ? o - L : (o < 0 ? o + L : o);
+        const int64_t q = q0 + w;
+        if (q < inner && o < Lout) out[(int64_t)o * inner + q] = v;
+    };
+    fft_ct<L, W, 256, INV>(smA, smB, tws, store);
+}
+
+template <int L, int W>
+__global__ void __launch_bounds__(256) k_fwd_x_ct(FwdXArgs a) {
+    extern __shared__ float2 sm[];
+    float2* smA = sm;
+    float2* smB = sm + L * W;
+    float2* tws = sm + 2 * L * W;
+    const int row0 = blockIdx.x * a.rows;
+    const int img = blockIdx.y;
+    const int c0 = blockIdx.z * a.cc;
+    const int nrows = a.Z * a.Y;
+    const int cc = a.cc;
+    const float2* __restrict__ src = a.img + (int64_t)img * a.img_stride;
+    for (int i = threadIdx.x; i < L; i += 256) tws[i] = a.tw[i];
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < L * W; idx += 256) {
+        const int m = idx / W, w = idx - m * W;
+        const int rl = w / cc, cl = w - rl * cc;
+        const int row = row0 + rl, c = c0 + cl;
+        int j = m + a.h;
+        if (j >= L) j -= L;
+        const int x = j - a.pad;
+        float2 v = make_float2(0.f, 0.f);
+        if (x >= 0 && x < a.X && row < nrows && c < a.C) {
+            const int z = row / a.Y, y = row - z * a.Y;
+            v = src[(int64_t)row * a.X + x];
+            if (a.maps) v = cmul(v, a.maps[((int64_t)row * a.X + x) * a.C + c]);
+            v = cscale(v, a.apz[z] * a.apy[y] * a.apx[x] * a.scale);
+        }
+        smA[idx] = v;
+    }
+    __syncthreads();
+    const int h = a.h;
+    auto store = [&](int k, int w, float2 v) {
+        const int rl = w / cc, cl = w - rl * cc;
+        const int row = row0 + rl, c = c0 + cl;
+        if (row >= nrows || c >= a.C) return;
+        int g = k + h;
+        if (g >= L) g -= L;
+        a.out[((int64_t)row * a.OSX + g) * a.ncol + (int64_t)img * a.C + c] = v;
+    };
+    fft_ct<L, W, 256, false>(smA, smB, tws, store);
+}
+
+template <int L, int W>
+__global__ void __launch_bounds__(256) k_adj_x_ct(AdjXArgs a) {
+    extern __shared__ float2 sm[];
+    float2* buf0 = sm;
+    float2* buf1 = sm + L * W;
+    float2* tws = sm + 2 * L * W;
+    float2* acc = tws + L;                  // [rows][X]
+    for (int i = threadIdx.x; i < L; i += 256) tws[i] = a.tw[i];
+    for (int i = threadIdx.x; i < a.rows * a.X; i += 256) acc[i] = make_float2(0.f, 0.f);
+    const int row0 = blockIdx.x * a.rows;
+    const int img = blockIdx.y;
+    const int nrows = a.Z * a.Y;
+    const int cc = a.cc;
+    float2* ep = fft_ct_free<L>(buf0, buf1);
+    const int shift = a.h - a.pad;
+    for (int c0 = 0; c0 < a.C; c0 += cc) {
+#pragma unroll 4
+        for (int idx = threadIdx.x; idx < L * W; idx += 256) {
+            const int m = idx / W, w = idx - m * W;
+            const int rl = w / cc, cl = w - rl * cc;
+            const int row = row0 + rl, c = c0 + cl;
+            int j = m + a.h;
+            if (j >= L) j -= L;
+            int bytes = 0;
+            const float2* g = a.in;
+            if (row < nrows && c < a.C) {
+                bytes = 8;
+                g = a.in + ((int64_t)row * a.OSX + j) * a.ncol + (int64_t)img * a.C + c;
+            }
+            cp_async8(buf0 + idx, g, bytes);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        const int X = a.X;
+        auto store = [&](int k, int w, float2 v) {
+            int o = k + shift;
+            o = o >= L ? o - L : (o < 0 ? o + L : o);
+            if (o < X) ep[o * W + w] = v;
+        };
+        fft_ct<L, W, 256, true>(buf0, buf1, tws, store);
+        __syncthreads();
+        for (int i = threadIdx.x; i < a.rows * X; i += 256) {
+            const int rl = i / X, x = i - rl * X;
+            const int row = row0 + rl;
+            if (row >= nrows) continue;
+            float2 s = acc[i];
+            for (int cl = 0; cl < cc && c0 + cl < a.C; ++cl) {
+                float2 v = ep[x * W + rl * cc + cl];
+                if (a.maps) v = cmulc(v, a.maps[((int64_t)row * X + x) * a.C + c0 + cl]);
+                s = cadd(s, v);
+            }
+            acc[i] = s;
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < a.rows * a.X; i += 256) {
+        const int rl = i / a.X, x = i - rl * a.X;
+        const int row = row0 + rl;
+        if (row >= nrows) continue;
+        const int z = row / a.Y, y = row - z * a.Y;
+        const float sc = a.apz[z] * a.apy[y] * a.apx[x] * a.scale;
+        float2 v = cscale(acc[i], sc);
+        float2* dst = a.img + (int64_t)img * a.img_stride + (int64_t)row * a.X + x;
+        if (a.accumulate) v = cadd(*dst, v);
+        *dst = v;
+    }
+}
+
 // ------------------------------------------------------------------ interpolation
 // G lanes cooperate on one sample (lane = column group); taps read ncol
 // contiguous complex values per grid point (coalesced across lanes).
@@ -349,6 +524,32 @@ __global__ void __launch_bounds__(256) k_interp(const float2* __restrict__ grid,
     float2 acc[CPL];
 #pragma unroll
     for (int j = 0; j < CPL; ++j) acc[j] = make_float2(0.f, 0.f);
+    if (wz[4] == 0.f && wy[4] == 0.f && wx[4] == 0.f) {
+        // common case: four taps per axis (k - 2 not an integer), fully unrolled
+#pragma unroll
+        for (int tz = 0; tz < 4; ++tz) {
+            const int64_t zoff = (int64_t)pmod(bz + tz, os0) * os1;
+#pragma unroll
+            for (int ty = 0; ty < 4; ++ty) {
+                const float wzy = wz[tz] * wy[ty];
+                const int64_t yoff = (zoff + iy[ty]) * os2;
+#pragma unroll
+                for (int tx = 0; tx < 4; ++tx) {
+                    const float w = wzy * wx[tx];
+                    const float2* gp = grid + (yoff + ix[tx]) * ncol;
+#pragma unroll
+                    for (int j = 0; j < CPL; ++j) {
+                        const int col = lane + j * G;
+                        if (col < ncol) {
+                            const float2 g = gp[col];
+                            acc[j].x += w * g.x;
+                            acc[j].y += w * g.y;
+                        }
+                    }
+                }
+            }
+        }
+    } else
 #pragma unroll 1
     for (int tz = 0; tz < 5; ++tz) {
         if (wz[tz] == 0.f) continue;
@@ -578,10 +779,12 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
         __syncthreads();
     }
     // ---- stage the tile in shared memory and write it out coalesced
+    // padded stride (ncc + 1) avoids bank conflicts across the 64 points
+    const int ps = ncc + 1;
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
         const int col = cs + 4 * j;
-        if (col < ncc) dq[p * ncc + col] = acc[j];
+        if (col < ncc) dq[p * ps + col] = acc[j];
     }
     __syncthreads();
     for (int i = tid; i < kTilePts * ncc; i += blockDim.x) {
@@ -589,7 +792,7 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
         const int qz = pp >> 4, qy = (pp >> 2) & 3, qx = pp & 3;
         if (qz >= Tz || qy >= Ty || qx >= Tx) continue;
         const int64_t g = ((int64_t)(t0z + qz) * a.os1 + (t0y + qy)) * a.os2 + (t0x + qx);
-        a.grid[g * a.ncol + col0 + col] = dq[i];
+        a.grid[g * a.ncol + col0 + col] = dq[pp * ps + col];
     }
 }
 
@@ -689,10 +892,18 @@ static tr_status launch_line(tr_plan* p, int axis, const float2* in, float2* out
     la.tw = A.twiddle;
     la.S = stages_of(A);
     const size_t smem = fft_smem_bytes(A.L, la.W);
-    TR_TRY(set_smem_limit((const void*)k_line, smem));
     dim3 grid((unsigned)((inner + la.W - 1) / la.W), (unsigned)outer);
-    k_line<<<grid, 256, smem, st>>>(la);
-    TR_CHECK_LAUNCH();
+    const void* fn = nullptr;
+    if (la.W == 16) {
+#define TR_LINE_CASE(LV)                                                                              \
+    case LV: fn = inv ? (const void*)k_line_ct<LV, 16, true> : (const void*)k_line_ct<LV, 16, false>; break;
+        switch (A.L) { TR_CT_LENGTHS(TR_LINE_CASE) default: break; }
+#undef TR_LINE_CASE
+    }
+    if (!fn) fn = (const void*)k_line;
+    TR_TRY(set_smem_limit(fn, smem));
+    void* args[] = {&la};
+    TR_CUDA(cudaLaunchKernel(fn, grid, dim3(256), args, smem, st));
     return TR_OK;
 }
 
@@ -726,10 +937,17 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
     fa.ncol = n_img * C;
     const int W = fa.rows * fa.cc;
     const size_t smem = fft_smem_bytes(OSX, W);
-    TR_TRY(set_smem_limit((const void*)k_fwd_x, smem));
     dim3 grid((unsigned)((Z * Y + fa.rows - 1) / fa.rows), (unsigned)n_img, (unsigned)((C + fa.cc - 1) / fa.cc));
-    k_fwd_x<<<grid, 256, smem, st>>>(fa);
-    TR_CHECK_LAUNCH();
+    const void* fn = nullptr;
+#define TR_FWDX_CASE(LV)                                                                    \
+    case LV: fn = (W == 16) ? (const void*)k_fwd_x_ct<LV, 16>                              \
+                            : (W == 12 ? (const void*)k_fwd_x_ct<LV, 12> : nullptr); break;
+    switch (OSX) { TR_CT_LENGTHS(TR_FWDX_CASE) default: break; }
+#undef TR_FWDX_CASE
+    if (!fn) fn = (const void*)k_fwd_x;
+    TR_TRY(set_smem_limit(fn, smem));
+    void* args[] = {&fa};
+    TR_CUDA(cudaLaunchKernel(fn, grid, dim3(256), args, smem, st));
     return TR_OK;
 }
 
@@ -772,7 +990,7 @@ static tr_status stage_interp(tr_plan* p, int bin, int ncol, int mode, float sig
 template <int CPT>
 static tr_status launch_spread_t(const SpreadArgs& sa, unsigned ntiles, unsigned nchunks, cudaStream_t st) {
     const size_t cand_bytes = (size_t)sa.K * (3 * 4 + 15 * 4 + 4 + 4) + 8;
-    const size_t dq_bytes = (size_t)std::max(sa.K, kTilePts) * sa.cchunk * sizeof(float2);
+    const size_t dq_bytes = (size_t)std::max(sa.K * sa.cchunk, kTilePts * (sa.cchunk + 1)) * sizeof(float2);
     const size_t smem = cand_bytes + dq_bytes;
     TR_TRY(set_smem_limit((const void*)k_spread<CPT>, smem));
     k_spread<CPT><<<dim3(ntiles, nchunks), 256, smem, st>>>(sa);
@@ -849,10 +1067,17 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
     aa.accumulate = 0;
     const int W = aa.rows * aa.cc;
     const size_t smem = fft_smem_bytes(OSX, W) + (size_t)aa.rows * X * sizeof(float2);
-    TR_TRY(set_smem_limit((const void*)k_adj_x, smem));
     dim3 grid((unsigned)((Z * Y + aa.rows - 1) / aa.rows), (unsigned)n_img);
-    k_adj_x<<<grid, 256, smem, st>>>(aa);
-    TR_CHECK_LAUNCH();
+    const void* fn = nullptr;
+#define TR_ADJX_CASE(LV)                                                                    \
+    case LV: fn = (W == 16) ? (const void*)k_adj_x_ct<LV, 16>                              \
+                            : (W == 12 ? (const void*)k_adj_x_ct<LV, 12> : nullptr); break;
+    switch (OSX) { TR_CT_LENGTHS(TR_ADJX_CASE) default: break; }
+#undef TR_ADJX_CASE
+    if (!fn) fn = (const void*)k_adj_x;
+    TR_TRY(set_smem_limit(fn, smem));
+    void* args[] = {&aa};
+    TR_CUDA(cudaLaunchKernel(fn, grid, dim3(256), args, smem, st));
     return TR_OK;
 }
 
