@@ -169,6 +169,27 @@ tr_status tr_power_iteration(tr_plan* plan, int32_t n_iter, void* work_images, d
  * Replaces the reference's wall-clock timers (tvme.py:509, :561-567). */
 tr_status tr_profile_nufft(tr_plan* plan, int32_t bin, int32_t reps, double* ms, double* bytes, void* stream);
 
+/* Allocation-free stopping-tolerance sums (no counterpart in the reference).
+ * For callers that cannot allocate device memory where they run the stopping
+ * test -- work enqueued while a stream is captured into a CUDA graph, or hosts
+ * that own the whole device heap -- this computes in FP64 what tr_pdhg_run's
+ * tolerance step computes, without a plan and without allocating:
+ *   TVM / TVME: sums_out = { sum |cur - prev|^2, sum |cur|^2 }
+ *   TVMW:       sums_out = { sum |prev - cur|^2, sum |prev|^2 }
+ * (tolerance = sqrt(s0) / sqrt(s1), resp. / max(sqrt(s1), 1e-12)).
+ * cur, prev: n complex64 values on the current device; sums_out: 2 doubles
+ * on the device, written asynchronously on `stream`.
+ * Limit: n <= TR_NOALLOC_MAX_ELEMS (larger n returns TR_ERR_INVALID_ARG).
+ * The partial sums live in a 64 KiB file-scope device array that every GPU
+ * loading the library keeps until exit; calls share it, so calls whose
+ * kernels may overlap on the GPU race and must be ordered by the caller.
+ * The first call on a device looks up that array's device address (a
+ * runtime call, no allocation); make that first call before any stream
+ * capture on the device. */
+#define TR_NOALLOC_MAX_ELEMS (64LL * 1024 * 1024)
+tr_status tr_tolerance_sums_noalloc(const void* cur, const void* prev, int64_t n, int32_t algorithm,
+                                    double* sums_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

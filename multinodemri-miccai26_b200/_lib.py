@@ -28,7 +28,7 @@ EXPORTED = (
     "tr_plan_create", "tr_plan_destroy", "tr_plan_info", "tr_last_error_string", "tr_plan_set_maps",
     "tr_plan_sort_kspace", "tr_plan_unsort_kspace", "tr_nufft_forward", "tr_nufft_adjoint",
     "tr_nufft_forward_bin", "tr_nufft_adjoint_bin", "tr_plan_bin_offset", "tr_pdhg_run",
-    "tr_power_iteration", "tr_profile_nufft",
+    "tr_power_iteration", "tr_profile_nufft", "tr_tolerance_sums_noalloc",
 )
 
 
@@ -124,6 +124,7 @@ def load() -> ctypes.CDLL:
             "tr_power_iteration": ([vp, i32, vp, ctypes.POINTER(ctypes.c_double), vp], i32),
             "tr_profile_nufft": ([vp, i32, i32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                   vp], i32),
+            "tr_tolerance_sums_noalloc": ([vp, vp, i64, i32, vp, vp], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(lib, name)
