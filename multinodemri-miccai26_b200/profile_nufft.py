@@ -35,6 +35,8 @@ def main(argv=None):
     ap.add_argument("--cones", type=int, default=700)
     ap.add_argument("--readout", type=int, default=600)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--pdhg", type=int, default=0, help="also run this many TVME iterations (all bins)")
+    ap.add_argument("--bins", type=int, default=2)
     args = ap.parse_args(argv)
     import torch
     syn = importlib.import_module(f"{PKG}.synthetic")
@@ -51,8 +53,26 @@ def main(argv=None):
     out = {"shape_zyx": list(shape), "os_shape": list(be.os_shape), "coils": args.coils, "echoes": args.echoes,
            "samples": int(coord.shape[0]), "stages": {k: {kk: round(vv, 4) for kk, vv in v.items()}
                                                       for k, v in prof.items()}}
-    print(json.dumps(out))
     be.close()
+    if args.pdhg:
+        solver = importlib.import_module(f"{PKG}.solver")
+        cfg = syn.SyntheticConfig("profile", shape, args.coils, args.echoes, args.bins, args.cones * args.bins,
+                                  args.readout, algorithm="tvme")
+        ds = syn.make_geometry(cfg)
+        syn.simulate_kspace_b200(ds, 0)
+        s = solver.PdhgSolver("tvme", shape, [ds.coord[ds.bin_indices(b)] for b in range(args.bins)], ds.bin_dcf(),
+                              ds.mps, ds.bin_ksp())
+        s.reset()
+        s.iterate(1, tol=0.0)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(s.stream)
+        s.iterate(args.pdhg, tol=0.0)
+        stop.record(s.stream)
+        stop.synchronize()
+        out["pdhg_ms_per_iteration"] = round(start.elapsed_time(stop) / args.pdhg, 4)
+        out["pdhg_bins"] = args.bins
+        s.close()
+    print(json.dumps(out))
 
 
 if __name__ == "__main__":
