@@ -98,6 +98,7 @@ struct tr_plan {
     int64_t total = 0;
     // device-resident trajectory (tile-sorted per bin)
     float4* ks = nullptr;        // (kz, ky, kx, dcf) in oversampled-grid units, sorted
+    void* taps = nullptr;        // per-sample first taps and KB weights (TapRec), sorted
     int32_t* perm = nullptr;     // sorted position -> acquisition index within the bin
     int32_t* tile_start = nullptr;  // per bin [ntiles + 1] (relative to the bin offset)
     int32_t* tile_order = nullptr;  // per bin [ntiles]: heaviest tiles first

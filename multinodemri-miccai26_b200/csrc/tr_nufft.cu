@@ -498,23 +498,199 @@ __global__ void __launch_bounds__(256) k_adj_x_ct(AdjXArgs a) {
     }
 }
 
+// ------------------------------------------------------------------ staged x-pass variants
+// W = 16 columns = ROWS image rows x CC coils (CC in {4, 8, 16}).  Forward:
+// each row's image values and its contiguous coil-map row are staged in shared
+// memory with cp.async, the products formed there.  Adjoint: the coil
+// combination runs with one thread per (x, coil) and a shuffle reduction over
+// the CC lanes of a coil group (no bank conflicts).
+template <int L, int CC>
+__global__ void __launch_bounds__(256) k_fwd_x_st(FwdXArgs a) {
+    constexpr int W = 16;
+    constexpr int ROWS = W / CC;
+    extern __shared__ float2 sm[];
+    float2* smA = sm;
+    float2* smB = sm + L * W;
+    float2* tws = sm + 2 * L * W;
+    const int X = a.X;
+    float2* s_img = smB;                 // [ROWS][X]
+    float2* s_map = smB + ROWS * X;      // [ROWS][X][CC]
+    __shared__ float s_apzy[ROWS];
+    const int row0 = blockIdx.x * ROWS;
+    const int img = blockIdx.y;
+    const int c0 = blockIdx.z * CC;
+    const int nrows = a.Z * a.Y;
+    const float2* __restrict__ src = a.img + (int64_t)img * a.img_stride;
+    for (int i = threadIdx.x; i < L; i += 256) tws[i] = a.tw[i];
+    if (threadIdx.x < ROWS) {
+        const int row = row0 + threadIdx.x;
+        float v = 0.f;
+        if (row < nrows) {
+            const int z = row / a.Y, y = row - z * a.Y;
+            v = a.apz[z] * a.apy[y] * a.scale;
+        }
+        s_apzy[threadIdx.x] = v;
+    }
+    for (int i = threadIdx.x; i < ROWS * X; i += 256) {
+        const int rl = i / X, x = i - rl * X;
+        const int row = row0 + rl;
+        cp_async8(s_img + i, row < nrows ? src + (int64_t)row * X + x : src, row < nrows ? 8 : 0);
+    }
+    if (a.maps) {
+        for (int i = threadIdx.x; i < ROWS * X * CC; i += 256) {
+            const int rl = i / (X * CC), rem = i - rl * X * CC;
+            const int x = rem / CC, cl = rem - x * CC;
+            const int row = row0 + rl, c = c0 + cl;
+            const bool ok = row < nrows && c < a.C;
+            cp_async8(s_map + i, ok ? a.maps + ((int64_t)row * X + x) * a.C + c : a.maps, ok ? 8 : 0);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < L * W; idx += 256) {
+        const int m = idx / W, w = idx - m * W;
+        const int rl = w / CC, cl = w - rl * CC;
+        int j = m + a.h;
+        if (j >= L) j -= L;
+        const int x = j - a.pad;
+        float2 v = make_float2(0.f, 0.f);
+        if (x >= 0 && x < X) {
+            v = s_img[rl * X + x];
+            if (a.maps) v = cmul(v, s_map[(rl * X + x) * CC + cl]);
+            v = cscale(v, s_apzy[rl] * a.apx[x]);
+        }
+        smA[idx] = v;
+    }
+    __syncthreads();
+    const int h = a.h;
+    auto store = [&](int k, int w, float2 v) {
+        const int rl = w / CC, cl = w - rl * CC;
+        const int row = row0 + rl, c = c0 + cl;
+        if (row >= nrows || c >= a.C) return;
+        int g = k + h;
+        if (g >= L) g -= L;
+        a.out[((int64_t)row * a.OSX + g) * a.ncol + (int64_t)img * a.C + c] = v;
+    };
+    fft_ct<L, W, 256, false>(smA, smB, tws, store);
+}
+
+template <int L, int CC>
+__global__ void __launch_bounds__(256) k_adj_x_st(AdjXArgs a) {
+    constexpr int W = 16;
+    constexpr int ROWS = W / CC;
+    extern __shared__ float2 sm[];
+    float2* buf0 = sm;
+    float2* buf1 = sm + L * W;
+    float2* tws = sm + 2 * L * W;
+    float2* acc = tws + L;                  // [ROWS][X]
+    for (int i = threadIdx.x; i < L; i += 256) tws[i] = a.tw[i];
+    for (int i = threadIdx.x; i < ROWS * a.X; i += 256) acc[i] = make_float2(0.f, 0.f);
+    const int row0 = blockIdx.x * ROWS;
+    const int img = blockIdx.y;
+    const int nrows = a.Z * a.Y;
+    const int X = a.X;
+    float2* ep = fft_ct_free<L>(buf0, buf1);
+    const int shift = a.h - a.pad;
+    for (int c0 = 0; c0 < a.C; c0 += CC) {
+#pragma unroll 4
+        for (int idx = threadIdx.x; idx < L * W; idx += 256) {
+            const int m = idx / W, w = idx - m * W;
+            const int rl = w / CC, cl = w - rl * CC;
+            const int row = row0 + rl, c = c0 + cl;
+            int j = m + a.h;
+            if (j >= L) j -= L;
+            const bool ok = row < nrows && c < a.C;
+            cp_async8(buf0 + idx, ok ? a.in + ((int64_t)row * a.OSX + j) * a.ncol + (int64_t)img * a.C + c : a.in,
+                      ok ? 8 : 0);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        auto store = [&](int k, int w, float2 v) {
+            int o = k + shift;
+            o = o >= L ? o - L : (o < 0 ? o + L : o);
+            if (o < X) ep[o * W + w] = v;
+        };
+        fft_ct<L, W, 256, true>(buf0, buf1, tws, store);
+        __syncthreads();
+        // thread (x, w): conj(S) product, then a sum over the CC lanes of one row.
+        // Every lane runs every iteration (the shuffles need the whole warp).
+        for (int base = 0; base < X * W; base += 256) {
+            const int i = base + (int)threadIdx.x;
+            const bool live = i < X * W;
+            const int x = i / W, w = i - x * W;
+            const int rl = w / CC, cl = w - rl * CC;
+            const int row = row0 + rl, c = c0 + cl;
+            float2 v = make_float2(0.f, 0.f);
+            if (live && row < nrows && c < a.C) {
+                v = ep[i];
+                if (a.maps) v = cmulc(v, a.maps[((int64_t)row * X + x) * a.C + c]);
+            }
+#pragma unroll
+            for (int o = CC / 2; o > 0; o >>= 1) {
+                v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+                v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+            }
+            if (live && cl == 0) acc[rl * X + x] = cadd(acc[rl * X + x], v);
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < ROWS * X; i += 256) {
+        const int rl = i / X, x = i - rl * X;
+        const int row = row0 + rl;
+        if (row >= nrows) continue;
+        const int z = row / a.Y, y = row - z * a.Y;
+        const float sc = a.apz[z] * a.apy[y] * a.apx[x] * a.scale;
+        float2 v = cscale(acc[i], sc);
+        float2* dst = a.img + (int64_t)img * a.img_stride + (int64_t)row * X + x;
+        if (a.accumulate) v = cadd(*dst, v);
+        *dst = v;
+    }
+}
+
+// ------------------------------------------------------------------ per-sample tap records
+// First tap per axis and the 15 KB weights of every (sorted) sample, computed
+// once at plan creation; interpolation and gridding read them instead of
+// re-evaluating the window.  w[0..4] z taps, w[5..9] y taps, w[10..14] x taps.
+struct __align__(16) TapRec {
+    int4 b;          // (bz, by, bx, 0): first tap on the oversampled grid (may be < 0)
+    float4 w[4];
+};
+
+__global__ void k_prep_taps(const float4* __restrict__ ks, int64_t M, float beta, TapRec* __restrict__ out) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= M) return;
+    const float4 k = ks[s];
+    float wz[5], wy[5], wx[5];
+    const int bz = axis_taps(k.x, beta, wz);
+    const int by = axis_taps(k.y, beta, wy);
+    const int bx = axis_taps(k.z, beta, wx);
+    TapRec r;
+    r.b = make_int4(bz, by, bx, 0);
+    r.w[0] = make_float4(wz[0], wz[1], wz[2], wz[3]);
+    r.w[1] = make_float4(wz[4], wy[0], wy[1], wy[2]);
+    r.w[2] = make_float4(wy[3], wy[4], wx[0], wx[1]);
+    r.w[3] = make_float4(wx[2], wx[3], wx[4], 0.f);
+    out[s] = r;
+}
+
 // ------------------------------------------------------------------ interpolation
 // G lanes cooperate on one sample (lane = column group); taps read ncol
 // contiguous complex values per grid point (coalesced across lanes).
 template <int CPL>
-__global__ void __launch_bounds__(256) k_interp(const float2* __restrict__ grid, const float4* __restrict__ ks,
-                                                int64_t M, int ncol, int G, int os0, int os1, int os2, float beta,
+__global__ void __launch_bounds__(256) k_interp(const float2* __restrict__ grid, const TapRec* __restrict__ taps,
+                                                int64_t M, int ncol, int G, int os0, int os1, int os2,
                                                 int mode, float sigma, const float2* __restrict__ y,
                                                 float2* __restrict__ out) {
     const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t s = gt / G;
     const int lane = (int)(gt - s * G);
     if (s >= M) return;
-    const float4 kk = ks[s];
-    float wz[5], wy[5], wx[5];
-    const int bz = axis_taps(kk.x, beta, wz);
-    const int by = axis_taps(kk.y, beta, wy);
-    const int bx = axis_taps(kk.z, beta, wx);
+    const TapRec rec = taps[s];
+    const float wz[5] = {rec.w[0].x, rec.w[0].y, rec.w[0].z, rec.w[0].w, rec.w[1].x};
+    const float wy[5] = {rec.w[1].y, rec.w[1].z, rec.w[1].w, rec.w[2].x, rec.w[2].y};
+    const float wx[5] = {rec.w[2].z, rec.w[2].w, rec.w[3].x, rec.w[3].y, rec.w[3].z};
+    const int bz = rec.b.x, by = rec.b.y, bx = rec.b.z;
     int iy[5], ix[5];
 #pragma unroll
     for (int t = 0; t < 5; ++t) {
@@ -593,17 +769,21 @@ __global__ void __launch_bounds__(256) k_interp(const float2* __restrict__ grid,
 }
 
 // ------------------------------------------------------------------ gridding (tile gather)
-// One CTA owns a 4x4x4 tile of the oversampled grid and all ncc columns of the
-// chunk.  Candidate samples come from the 27 neighbouring tiles of the sorted
-// trajectory; those whose support meets the tile are compacted (in candidate
-// order) with their per-axis weights, their values staged in shared memory,
-// and every (point, column) accumulator sums over them in that fixed order.
-// No atomics: the result is bitwise reproducible.
+// One CTA owns a 4x4x4 tile of the oversampled grid and up to 16*CG columns.
+// Thread (row, g): row = (pz, py) of the tile (16 rows, each 4 x-points),
+// g = column group of CG consecutive columns.  Candidate samples come from
+// the home tiles that can reach the tile; 256 are tested per round and the
+// ones whose support meets the tile are compacted in candidate order (block
+// prefix sum, no atomics); their weights and weighted values are staged in
+// shared memory 64 at a time and every (point, column) accumulator sums them
+// in that fixed order.  Bitwise reproducible.
 constexpr int kTile = 4;
-constexpr int kTilePts = kTile * kTile * kTile;
+constexpr int kSpreadRound = 256;   // candidates tested per round
+constexpr int kSpreadSub = 64;      // candidates staged per sub-chunk
 
 struct SpreadArgs {
-    const float4* ks;          // bin base
+    const float4* ks;          // bin base (dcf in .w)
+    const TapRec* taps;        // bin base
     const int32_t* tile_start; // bin base [ntiles + 1]
     const int32_t* tile_order; // bin base [ntiles] or null
     const float2* vals;        // (M_b, ncol) bin base
@@ -612,11 +792,16 @@ struct SpreadArgs {
     float2* grid;              // (OSZ, OSY, OSX, ncol)
     int os0, os1, os2;
     int nt0, nt1, nt2;
-    float beta;
-    int K;                     // candidates per chunk
 };
 
-template <int CPT>
+__device__ __forceinline__ int wrap_rel(int t0, int b0, int os) {
+    // (t0 - b0) mod os mapped to (-os + 4, 4]: the tap index of point t0
+    int r = pmod(t0 - b0, os);
+    if (r > 4) r -= os;
+    return r;
+}
+
+template <int CG>
 __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ int run_start[64];
@@ -625,12 +810,10 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
     __shared__ int tlist[3][4];
     __shared__ int warp_cnt[8];
     __shared__ int warp_off[9];
-    const int K = a.K;
-    int* c_rel = reinterpret_cast<int*>(smraw);                  // [K][3]
-    float* c_w = reinterpret_cast<float*>(c_rel + 3 * K);        // [K][15]
-    int* c_s = reinterpret_cast<int*>(c_w + 15 * K);             // [K]
-    float* c_d = reinterpret_cast<float*>(c_s + K);              // [K]
-    float2* dq = reinterpret_cast<float2*>(c_d + K);             // [max(K, 64)][ncc] (80 K bytes in: 8-aligned)
+    __shared__ int l_s[kSpreadRound];        // compacted sample indices
+    __shared__ int l_rel[kSpreadRound];      // packed tap offsets of the tile origin
+    float* c_w = reinterpret_cast<float*>(smraw);                        // [kSpreadSub][16]
+    float2* dq = reinterpret_cast<float2*>(c_w + 16 * kSpreadSub);       // [kSpreadSub][ncc]
 
     const int col0 = blockIdx.y * a.cchunk;
     const int ncc = min(a.cchunk, a.ncol - col0);
@@ -641,11 +824,11 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
     const int tx = trem - ty * a.nt2;
     const int t0z = tz * kTile, t0y = ty * kTile, t0x = tx * kTile;
     const int Tz = min(kTile, a.os0 - t0z), Ty = min(kTile, a.os1 - t0y), Tx = min(kTile, a.os2 - t0x);
-
     const int tid = threadIdx.x;
-    // Home tiles that can reach this tile: per axis, the distinct tiles holding
-    // floor(k) in [t0 - 2, t0 + T + 1] (wrapped).  At most four per axis when
-    // the last tile of the axis is shorter than the kernel reach.
+    const int lane = tid & 31, warp = tid >> 5;
+
+    // home tiles that can reach this tile: per axis the distinct tiles holding
+    // floor(k) in [t0 - 2, t0 + T + 1] (wrapped); at most four per axis
     if (tid < 3) {
         const int t0 = tid == 0 ? t0z : (tid == 1 ? t0y : t0x);
         const int Tn = tid == 0 ? Tz : (tid == 1 ? Ty : Tx);
@@ -673,54 +856,50 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
         run_pref[tid + 1] = a.tile_start[id + 1] - a.tile_start[id];
     }
     __syncthreads();
-    if (tid == 0) {
-        run_pref[0] = 0;
-        for (int r = 0; r < nruns; ++r) run_pref[r + 1] += run_pref[r];
+    if (tid < 32) {   // inclusive scan of the run lengths by one warp
+        int carry = 0;
+        for (int b0 = 0; b0 < nruns; b0 += 32) {
+            int v = (b0 + lane < nruns) ? run_pref[b0 + lane + 1] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += t;
+            }
+            if (b0 + lane < nruns) run_pref[b0 + lane + 1] = v + carry;
+            carry += __shfl_sync(0xffffffffu, v, 31);
+        }
+        if (lane == 0) run_pref[0] = 0;
     }
     __syncthreads();
     const int total = run_pref[nruns];
-    if (total == 0) {   // empty neighbourhood: the tile is zero
-        for (int i = tid; i < kTilePts * ncc; i += blockDim.x) {
-            const int pp = i / ncc, col = i - pp * ncc;
-            const int qz = pp >> 4, qy = (pp >> 2) & 3, qx = pp & 3;
-            if (qz >= Tz || qy >= Ty || qx >= Tx) continue;
-            const int64_t g = ((int64_t)(t0z + qz) * a.os1 + (t0y + qy)) * a.os2 + (t0x + qx);
-            a.grid[g * a.ncol + col0 + col] = make_float2(0.f, 0.f);
-        }
-        return;
-    }
 
-    const int p = tid & 63;
-    const int pz = p >> 4, py = (p >> 2) & 3, px = p & 3;
-    const int cs = tid >> 6;
-    float2 acc[CPT];
+    const int row = tid >> 4;
+    const int pz = row >> 2, py = row & 3;
+    const int g = tid & 15;
+    const int c_lo = g * CG;
+    float2 acc[4][CG];
 #pragma unroll
-    for (int j = 0; j < CPT; ++j) acc[j] = make_float2(0.f, 0.f);
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+        for (int j = 0; j < CG; ++j) acc[x][j] = make_float2(0.f, 0.f);
 
-    const int lane = tid & 31, warp = tid >> 5;
-    for (int base = 0; base < total; base += K) {
-        // ---- phase 1: candidate test and deterministic compaction
-        int flag = 0, rel[3] = {0, 0, 0}, sidx = 0;
-        float4 kk = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int base = 0; base < total; base += kSpreadRound) {
+        // ---- test 256 candidates and compact the ones meeting the tile
+        int flag = 0, sidx = 0, packed = 0;
         const int ci = base + tid;
-        if (tid < K && ci < total) {
-            int r = 0;
-            while (run_pref[r + 1] <= ci) ++r;
-            sidx = run_start[r] + (ci - run_pref[r]);
-            kk = a.ks[sidx];
-            const float kc[3] = {kk.x, kk.y, kk.z};
-            const int t0[3] = {t0z, t0y, t0x};
-            const int Tn[3] = {Tz, Ty, Tx};
-            const int osn[3] = {a.os0, a.os1, a.os2};
-            flag = 1;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const int b0 = (int)ceil((double)kc[d] - 2.0);
-                int rr = pmod(t0[d] - b0, osn[d]);
-                if (rr > 4) rr -= osn[d];
-                rel[d] = rr;
-                if (rr > 4 || rr + Tn[d] - 1 < 0) flag = 0;
+        if (ci < total) {
+            int lo = 0, hi = nruns - 1;          // run r with pref[r] <= ci < pref[r+1]
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (run_pref[mid] <= ci) lo = mid; else hi = mid - 1;
             }
+            sidx = run_start[lo] + (ci - run_pref[lo]);
+            const int4 b = a.taps[sidx].b;
+            const int rz = wrap_rel(t0z, b.x, a.os0);
+            const int ry = wrap_rel(t0y, b.y, a.os1);
+            const int rx = wrap_rel(t0x, b.z, a.os2);
+            flag = (rz + Tz - 1 >= 0) && (ry + Ty - 1 >= 0) && (rx + Tx - 1 >= 0);
+            packed = ((rz + 128) & 0xff) | (((ry + 128) & 0xff) << 8) | (((rx + 128) & 0xff) << 16);
         }
         const unsigned bal = __ballot_sync(0xffffffffu, flag);
         if (lane == 0) warp_cnt[warp] = __popc(bal);
@@ -730,69 +909,66 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
             for (int w = 0; w < 8; ++w) warp_off[w + 1] = warp_off[w] + warp_cnt[w];
         }
         __syncthreads();
-        const int nc = warp_off[8];
+        const int nl = warp_off[8];
         if (flag) {
             const int pos = warp_off[warp] + __popc(bal & ((1u << lane) - 1u));
-            c_rel[3 * pos + 0] = rel[0];
-            c_rel[3 * pos + 1] = rel[1];
-            c_rel[3 * pos + 2] = rel[2];
-            float w5[5];
-            axis_taps(kk.x, a.beta, w5);
-#pragma unroll
-            for (int t = 0; t < 5; ++t) c_w[15 * pos + t] = w5[t];
-            axis_taps(kk.y, a.beta, w5);
-#pragma unroll
-            for (int t = 0; t < 5; ++t) c_w[15 * pos + 5 + t] = w5[t];
-            axis_taps(kk.z, a.beta, w5);
-#pragma unroll
-            for (int t = 0; t < 5; ++t) c_w[15 * pos + 10 + t] = w5[t];
-            c_s[pos] = sidx;
-            c_d[pos] = a.use_dcf ? kk.w : 1.0f;
+            l_s[pos] = sidx;
+            l_rel[pos] = packed;
         }
         __syncthreads();
-        // ---- phase 2: stage weighted values
-        for (int i = tid; i < nc * ncc; i += blockDim.x) {
-            const int cand = i / ncc, col = i - cand * ncc;
-            float2 v = a.vals[(int64_t)c_s[cand] * a.ncol + col0 + col];
-            dq[i] = cscale(v, c_d[cand]);
-        }
-        __syncthreads();
-        // ---- phase 3: gather-accumulate in candidate order
-        for (int cc = 0; cc < nc; ++cc) {
-            const int az = c_rel[3 * cc + 0] + pz;
-            const int ay = c_rel[3 * cc + 1] + py;
-            const int ax = c_rel[3 * cc + 2] + px;
-            if ((unsigned)az > 4u || (unsigned)ay > 4u || (unsigned)ax > 4u) continue;
-            const float w = c_w[15 * cc + az] * c_w[15 * cc + 5 + ay] * c_w[15 * cc + 10 + ax];
-            if (w == 0.f) continue;
-            const float2* row = dq + cc * ncc;
+        // ---- accumulate the compacted list, kSpreadSub candidates at a time
+        for (int sub = 0; sub < nl; sub += kSpreadSub) {
+            const int ns = min(kSpreadSub, nl - sub);
+            if (tid < 4 * ns) {
+                const int cand = tid >> 2, part = tid & 3;
+                reinterpret_cast<float4*>(c_w)[cand * 4 + part] = a.taps[l_s[sub + cand]].w[part];
+            }
+            for (int i = tid; i < ns * ncc; i += 256) {
+                const int cand = i / ncc, col = i - cand * ncc;
+                const int sm = l_s[sub + cand];
+                float2 v = a.vals[(int64_t)sm * a.ncol + col0 + col];
+                if (a.use_dcf) v = cscale(v, a.ks[sm].w);
+                dq[i] = v;
+            }
+            __syncthreads();
+            for (int cc = 0; cc < ns; ++cc) {
+                const int pk = l_rel[sub + cc];
+                const int az = (pk & 0xff) - 128 + pz;
+                const int ay = ((pk >> 8) & 0xff) - 128 + py;
+                if ((unsigned)az > 4u || (unsigned)ay > 4u) continue;
+                const float* w = c_w + 16 * cc;
+                const float wzy = w[az] * w[5 + ay];
+                if (wzy == 0.f) continue;
+                const int rx = ((pk >> 16) & 0xff) - 128;
+                float2 v[CG];
 #pragma unroll
-            for (int j = 0; j < CPT; ++j) {
-                const int col = cs + 4 * j;
-                if (col < ncc) {
-                    const float2 v = row[col];
-                    acc[j].x += w * v.x;
-                    acc[j].y += w * v.y;
+                for (int j = 0; j < CG; ++j) v[j] = (c_lo + j < ncc) ? dq[cc * ncc + c_lo + j] : make_float2(0.f, 0.f);
+#pragma unroll
+                for (int x = 0; x < 4; ++x) {
+                    const int ax = rx + x;
+                    if ((unsigned)ax > 4u) continue;
+                    const float wt = wzy * w[10 + ax];
+#pragma unroll
+                    for (int j = 0; j < CG; ++j) {
+                        acc[x][j].x += wt * v[j].x;
+                        acc[x][j].y += wt * v[j].y;
+                    }
                 }
             }
+            __syncthreads();
         }
-        __syncthreads();
     }
-    // ---- stage the tile in shared memory and write it out coalesced
-    // padded stride (ncc + 1) avoids bank conflicts across the 64 points
-    const int ps = ncc + 1;
+    // ---- write the tile: each thread its 4 x-points x CG columns
+    if (pz < Tz && py < Ty) {
+        const int64_t rowg = ((int64_t)(t0z + pz) * a.os1 + (t0y + py)) * a.os2 + t0x;
 #pragma unroll
-    for (int j = 0; j < CPT; ++j) {
-        const int col = cs + 4 * j;
-        if (col < ncc) dq[p * ps + col] = acc[j];
-    }
-    __syncthreads();
-    for (int i = tid; i < kTilePts * ncc; i += blockDim.x) {
-        const int pp = i / ncc, col = i - pp * ncc;
-        const int qz = pp >> 4, qy = (pp >> 2) & 3, qx = pp & 3;
-        if (qz >= Tz || qy >= Ty || qx >= Tx) continue;
-        const int64_t g = ((int64_t)(t0z + qz) * a.os1 + (t0y + qy)) * a.os2 + (t0x + qx);
-        a.grid[g * a.ncol + col0 + col] = dq[pp * ps + col];
+        for (int x = 0; x < 4; ++x) {
+            if (x >= Tx) continue;
+            float2* dst = a.grid + (rowg + x) * a.ncol + col0 + c_lo;
+#pragma unroll
+            for (int j = 0; j < CG; ++j)
+                if (c_lo + j < ncc) dst[j] = acc[x][j];
+        }
     }
 }
 
@@ -939,9 +1115,16 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
     const size_t smem = fft_smem_bytes(OSX, W);
     dim3 grid((unsigned)((Z * Y + fa.rows - 1) / fa.rows), (unsigned)n_img, (unsigned)((C + fa.cc - 1) / fa.cc));
     const void* fn = nullptr;
-#define TR_FWDX_CASE(LV)                                                                    \
-    case LV: fn = (W == 16) ? (const void*)k_fwd_x_ct<LV, 16>                              \
-                            : (W == 12 ? (const void*)k_fwd_x_ct<LV, 12> : nullptr); break;
+    // staged variant when a row's coil-map slice fits the free FFT buffer
+    const bool staged = (W == 16) && (fa.cc == 16 || fa.cc == 8 || fa.cc == 4) &&
+                        (size_t)(16 / fa.cc) * X * (fa.cc + 1) <= (size_t)OSX * 16;
+#define TR_FWDX_CASE(LV)                                                                        \
+    case LV:                                                                                    \
+        if (staged) fn = fa.cc == 16 ? (const void*)k_fwd_x_st<LV, 16>                          \
+                       : (fa.cc == 8 ? (const void*)k_fwd_x_st<LV, 8> : (const void*)k_fwd_x_st<LV, 4>); \
+        else fn = (W == 16) ? (const void*)k_fwd_x_ct<LV, 16>                                   \
+                            : (W == 12 ? (const void*)k_fwd_x_ct<LV, 12> : nullptr);            \
+        break;
     switch (OSX) { TR_CT_LENGTHS(TR_FWDX_CASE) default: break; }
 #undef TR_FWDX_CASE
     if (!fn) fn = (const void*)k_fwd_x;
@@ -972,10 +1155,10 @@ static tr_status stage_interp(tr_plan* p, int bin, int ncol, int mode, float sig
     const int cpl = (ncol + G - 1) / G;
     const int64_t threads = b.count * G;
     const unsigned blocks = (unsigned)((threads + 255) / 256);
-    const float4* ks = p->ks + b.offset;
-#define TR_INTERP(CPLV)                                                                                        \
-    k_interp<CPLV><<<blocks, 256, 0, st>>>(p->bufA, ks, b.count, ncol, G, p->os[0], p->os[1], p->os[2], p->beta, \
-                                           mode, sigma, y, out)
+    const TapRec* taps = reinterpret_cast<const TapRec*>(p->taps) + b.offset;
+#define TR_INTERP(CPLV)                                                                                      \
+    k_interp<CPLV><<<blocks, 256, 0, st>>>(p->bufA, taps, b.count, ncol, G, p->os[0], p->os[1], p->os[2], mode, \
+                                           sigma, y, out)
     if (cpl <= 1) TR_INTERP(1);
     else if (cpl <= 2) TR_INTERP(2);
     else if (cpl <= 3) TR_INTERP(3);
@@ -987,27 +1170,27 @@ static tr_status stage_interp(tr_plan* p, int bin, int ncol, int mode, float sig
     return TR_OK;
 }
 
-template <int CPT>
+template <int CG>
 static tr_status launch_spread_t(const SpreadArgs& sa, unsigned ntiles, unsigned nchunks, cudaStream_t st) {
-    const size_t cand_bytes = (size_t)sa.K * (3 * 4 + 15 * 4 + 4 + 4) + 8;
-    const size_t dq_bytes = (size_t)std::max(sa.K * sa.cchunk, kTilePts * (sa.cchunk + 1)) * sizeof(float2);
-    const size_t smem = cand_bytes + dq_bytes;
-    TR_TRY(set_smem_limit((const void*)k_spread<CPT>, smem));
-    k_spread<CPT><<<dim3(ntiles, nchunks), 256, smem, st>>>(sa);
+    const size_t smem = (size_t)kSpreadSub * 16 * sizeof(float) + (size_t)kSpreadSub * sa.cchunk * sizeof(float2);
+    TR_TRY(set_smem_limit((const void*)k_spread<CG>, smem));
+    k_spread<CG><<<dim3(ntiles, nchunks), 256, smem, st>>>(sa);
     TR_CHECK_LAUNCH();
     return TR_OK;
 }
 
-// gridding: one CTA per (4x4x4 tile, chunk of <= 32 columns)
+// gridding: one CTA per (4x4x4 tile, chunk of <= 128 columns)
 static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, bool use_dcf, cudaStream_t st) {
     const Bin& b = p->bins[bin];
     SpreadArgs sa;
     sa.ks = p->ks + b.offset;
+    sa.taps = reinterpret_cast<const TapRec*>(p->taps) + b.offset;
     sa.tile_start = p->tile_start + (int64_t)bin * (p->ntiles + 1);
     sa.tile_order = p->tile_order + (int64_t)bin * p->ntiles;
     sa.vals = ksp;
     sa.ncol = ncol;
-    sa.cchunk = std::min(32, ncol);
+    const int nch = (ncol + 127) / 128;
+    sa.cchunk = (ncol + nch - 1) / nch;
     sa.use_dcf = (use_dcf && p->has_dcf) ? 1 : 0;
     sa.grid = p->bufA;
     sa.os0 = p->os[0];
@@ -1016,14 +1199,12 @@ static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, 
     sa.nt0 = p->ntile[0];
     sa.nt1 = p->ntile[1];
     sa.nt2 = p->ntile[2];
-    sa.beta = p->beta;
-    sa.K = 128;
-    const int cpt = (sa.cchunk + 3) / 4;
+    const int cg = (sa.cchunk + 15) / 16;
     const unsigned nt = (unsigned)p->ntiles;
-    const unsigned nch = (unsigned)((ncol + sa.cchunk - 1) / sa.cchunk);
-    if (cpt <= 1) return launch_spread_t<1>(sa, nt, nch, st);
-    if (cpt <= 2) return launch_spread_t<2>(sa, nt, nch, st);
-    if (cpt <= 4) return launch_spread_t<4>(sa, nt, nch, st);
+    if (cg <= 1) return launch_spread_t<1>(sa, nt, nch, st);
+    if (cg <= 2) return launch_spread_t<2>(sa, nt, nch, st);
+    if (cg <= 4) return launch_spread_t<4>(sa, nt, nch, st);
+    if (cg <= 6) return launch_spread_t<6>(sa, nt, nch, st);
     return launch_spread_t<8>(sa, nt, nch, st);
 }
 
@@ -1069,9 +1250,15 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
     const size_t smem = fft_smem_bytes(OSX, W) + (size_t)aa.rows * X * sizeof(float2);
     dim3 grid((unsigned)((Z * Y + aa.rows - 1) / aa.rows), (unsigned)n_img);
     const void* fn = nullptr;
-#define TR_ADJX_CASE(LV)                                                                    \
-    case LV: fn = (W == 16) ? (const void*)k_adj_x_ct<LV, 16>                              \
-                            : (W == 12 ? (const void*)k_adj_x_ct<LV, 12> : nullptr); break;
+    const bool pow2 = (W == 16) && (aa.cc == 16 || aa.cc == 8 || aa.cc == 4 || aa.cc == 2 || aa.cc == 1);
+#define TR_ADJX_CASE(LV)                                                                        \
+    case LV:                                                                                    \
+        if (pow2) fn = aa.cc == 16 ? (const void*)k_adj_x_st<LV, 16>                            \
+                     : aa.cc == 8 ? (const void*)k_adj_x_st<LV, 8>                              \
+                     : aa.cc == 4 ? (const void*)k_adj_x_st<LV, 4>                              \
+                     : aa.cc == 2 ? (const void*)k_adj_x_st<LV, 2> : (const void*)k_adj_x_st<LV, 1>; \
+        else fn = (W == 12 ? (const void*)k_adj_x_ct<LV, 12> : nullptr);                        \
+        break;
     switch (OSX) { TR_CT_LENGTHS(TR_ADJX_CASE) default: break; }
 #undef TR_ADJX_CASE
     if (!fn) fn = (const void*)k_adj_x;
@@ -1185,6 +1372,7 @@ static void plan_free(tr_plan* p) {
         cudaFree(a.apod);
     }
     cudaFree(p->ks);
+    cudaFree(p->taps);
     cudaFree(p->perm);
     cudaFree(p->tile_start);
     cudaFree(p->tile_order);
@@ -1356,18 +1544,22 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
     }
     const size_t nks = (size_t)std::max<int64_t>(off, 1);
     if (cudaMalloc(&p->ks, nks * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc(&p->taps, nks * sizeof(TapRec)) != cudaSuccess ||
         cudaMalloc(&p->perm, nks * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&p->tile_start, tstart.size() * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&p->tile_order, torder.size() * sizeof(int32_t)) != cudaSuccess)
         return bad(TR_ERR_OOM, "allocation of the sorted trajectory failed");
     TR_CUDA(cudaMemcpy(p->ks, ks_sorted.data(), nks * sizeof(float4), cudaMemcpyHostToDevice));
     TR_CUDA(cudaMemcpy(p->perm, perm.data(), nks * sizeof(int32_t), cudaMemcpyHostToDevice));
+    k_prep_taps<<<(unsigned)((nks + 255) / 256), 256>>>(p->ks, (int64_t)nks, p->beta, (TapRec*)p->taps);
+    TR_CHECK_LAUNCH();
+    TR_CUDA(cudaDeviceSynchronize());
     TR_CUDA(cudaMemcpy(p->tile_start, tstart.data(), tstart.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     TR_CUDA(cudaMemcpy(p->tile_order, torder.data(), torder.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     if (cudaMalloc(&p->tol_dev, 4 * sizeof(double)) != cudaSuccess ||
         cudaMallocHost(&p->tol_host, 4 * sizeof(double)) != cudaSuccess)
         return bad(TR_ERR_OOM, "allocation of reduction scalars failed");
-    p->workspace_bytes = (int64_t)(nks * (sizeof(float4) + sizeof(int32_t)) +
+    p->workspace_bytes = (int64_t)(nks * (sizeof(float4) + sizeof(TapRec) + sizeof(int32_t)) +
                                    (tstart.size() + torder.size()) * sizeof(int32_t));
     TR_TRY(wavelet_prepare(p));
     *out = p;

@@ -110,7 +110,8 @@ def test_adjoint_is_bitwise_deterministic():
 
 @pytest.mark.parametrize("shape,E,C", [((12, 16, 20), 1, 1), ((12, 16, 20), 2, 3), ((12, 16, 20), 3, 16),
                                        ((12, 16, 20), 6, 16), ((48, 64, 64), 2, 16), ((48, 64, 64), 2, 12),
-                                       ((48, 64, 64), 3, 6), ((48, 64, 64), 1, 40)])
+                                       ((48, 64, 64), 3, 6), ((48, 64, 64), 1, 40), ((48, 64, 64), 2, 8),
+                                       ((48, 64, 64), 3, 4), ((48, 64, 64), 1, 1), ((50, 64, 64), 2, 16)])
 def test_batched_coil_echo_path(shape, E, C):
     torch = _torch()
     nb = pkg("nufft_backend")
