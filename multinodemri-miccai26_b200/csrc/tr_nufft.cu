@@ -326,7 +326,12 @@ __global__ void __launch_bounds__(256) k_adj_x(AdjXArgs a) {
 // ------------------------------------------------------------------ compile-time variants
 // The same three FFT kernels with L and W fixed at compile time (fft_ct):
 // used for the transform lengths of the supported workloads.
-#define TR_CT_LENGTHS(X) X(60) X(80) X(100) X(120) X(140) X(160) X(200) X(240) X(320)
+// Lengths up to 200 use 16-column tiles, longer ones 8-column tiles (the
+// shared-memory footprint 2 L W x 8 bytes then allows >= 4 CTAs per SM).
+#define TR_CT_WIDE(X) X(60) X(80) X(100) X(120) X(140) X(160) X(200)
+#define TR_CT_NARROW(X) X(240) X(320)
+#define TR_CT_LENGTHS(X) TR_CT_WIDE(X) TR_CT_NARROW(X)
+__host__ __device__ constexpr int ct_width(int L) { return L >= 240 ? 8 : 16; }
 
 template <int L, int W, bool INV>
 __global__ void __launch_bounds__(256) k_line_ct(LineArgs a) {
@@ -504,9 +509,8 @@ __global__ void __launch_bounds__(256) k_adj_x_ct(AdjXArgs a) {
 // memory with cp.async, the products formed there.  Adjoint: the coil
 // combination runs with one thread per (x, coil) and a shuffle reduction over
 // the CC lanes of a coil group (no bank conflicts).
-template <int L, int CC>
+template <int L, int W, int CC>
 __global__ void __launch_bounds__(256) k_fwd_x_st(FwdXArgs a) {
-    constexpr int W = 16;
     constexpr int ROWS = W / CC;
     extern __shared__ float2 sm[];
     float2* smA = sm;
@@ -575,9 +579,8 @@ __global__ void __launch_bounds__(256) k_fwd_x_st(FwdXArgs a) {
     fft_ct<L, W, 256, false>(smA, smB, tws, store);
 }
 
-template <int L, int CC>
+template <int L, int W, int CC>
 __global__ void __launch_bounds__(256) k_adj_x_st(AdjXArgs a) {
-    constexpr int W = 16;
     constexpr int ROWS = W / CC;
     extern __shared__ float2 sm[];
     float2* buf0 = sm;
@@ -1067,16 +1070,18 @@ static tr_status launch_line(tr_plan* p, int axis, const float2* in, float2* out
     la.inv = inv;
     la.tw = A.twiddle;
     la.S = stages_of(A);
+    const void* fn = nullptr;
+#define TR_LINE_CASE(LV)                                                                                  \
+    case LV:                                                                                              \
+        la.W = ct_width(LV);                                                                              \
+        fn = inv ? (const void*)k_line_ct<LV, ct_width(LV), true> : (const void*)k_line_ct<LV, ct_width(LV), false>; \
+        break;
+    switch (A.L) { TR_CT_LENGTHS(TR_LINE_CASE) default: break; }
+#undef TR_LINE_CASE
+    if (!fn) fn = (const void*)k_line;
+    la.vec16 = ((inner % 2) == 0 && (la.W % 2) == 0 && ((uintptr_t)in % 16) == 0) ? 1 : 0;
     const size_t smem = fft_smem_bytes(A.L, la.W);
     dim3 grid((unsigned)((inner + la.W - 1) / la.W), (unsigned)outer);
-    const void* fn = nullptr;
-    if (la.W == 16) {
-#define TR_LINE_CASE(LV)                                                                              \
-    case LV: fn = inv ? (const void*)k_line_ct<LV, 16, true> : (const void*)k_line_ct<LV, 16, false>; break;
-        switch (A.L) { TR_CT_LENGTHS(TR_LINE_CASE) default: break; }
-#undef TR_LINE_CASE
-    }
-    if (!fn) fn = (const void*)k_line;
     TR_TRY(set_smem_limit(fn, smem));
     void* args[] = {&la};
     TR_CUDA(cudaLaunchKernel(fn, grid, dim3(256), args, smem, st));
@@ -1101,8 +1106,20 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
     fa.OSX = OSX;
     fa.h = p->ax[2].h;
     fa.pad = p->ax[2].pad;
-    fa.cc = coils_per_cta(C);
-    fa.rows = std::max(1, 16 / fa.cc);
+    // launch shape: compile-time kernels for the listed lengths
+    bool ct = false;
+#define TR_IS_CT(LV) case LV: ct = true; break;
+    switch (OSX) { TR_CT_LENGTHS(TR_IS_CT) default: break; }
+#undef TR_IS_CT
+    const int Wct = ct_width(OSX);
+    const bool pow2C = (C & (C - 1)) == 0;
+    if (ct && (C >= Wct || pow2C)) {
+        fa.cc = C >= Wct ? Wct : C;
+        fa.rows = Wct / fa.cc;
+    } else {
+        fa.cc = coils_per_cta(C);
+        fa.rows = std::max(1, 16 / fa.cc);
+    }
     fa.apz = p->ax[0].apod;
     fa.apy = p->ax[1].apod;
     fa.apx = p->ax[2].apod;
@@ -1116,15 +1133,16 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
     dim3 grid((unsigned)((Z * Y + fa.rows - 1) / fa.rows), (unsigned)n_img, (unsigned)((C + fa.cc - 1) / fa.cc));
     const void* fn = nullptr;
     // staged variant when a row's coil-map slice fits the free FFT buffer
-    const bool staged = (W == 16) && (fa.cc == 16 || fa.cc == 8 || fa.cc == 4) &&
-                        (size_t)(16 / fa.cc) * X * (fa.cc + 1) <= (size_t)OSX * 16;
-#define TR_FWDX_CASE(LV)                                                                        \
-    case LV:                                                                                    \
-        if (staged) fn = fa.cc == 16 ? (const void*)k_fwd_x_st<LV, 16>                          \
-                       : (fa.cc == 8 ? (const void*)k_fwd_x_st<LV, 8> : (const void*)k_fwd_x_st<LV, 4>); \
-        else fn = (W == 16) ? (const void*)k_fwd_x_ct<LV, 16>                                   \
-                            : (W == 12 ? (const void*)k_fwd_x_ct<LV, 12> : nullptr);            \
-        break;
+    const bool staged = ct && W == Wct && fa.cc >= 4 && (size_t)fa.rows * X * (fa.cc + 1) <= (size_t)OSX * W;
+#define TR_FWDX_CASE(LV)                                                                              \
+    case LV: {                                                                                        \
+        constexpr int WV = ct_width(LV);                                                              \
+        if (staged) fn = fa.cc == 16 ? (const void*)k_fwd_x_st<LV, WV, (WV >= 16 ? 16 : WV)>          \
+                       : fa.cc == 8 ? (const void*)k_fwd_x_st<LV, WV, 8> : (const void*)k_fwd_x_st<LV, WV, 4>; \
+        else if (W == WV) fn = (const void*)k_fwd_x_ct<LV, WV>;                                       \
+        else if (W == 12 && WV == 16) fn = (const void*)k_fwd_x_ct<LV, 12>;                          \
+        break;                                                                                        \
+    }
     switch (OSX) { TR_CT_LENGTHS(TR_FWDX_CASE) default: break; }
 #undef TR_FWDX_CASE
     if (!fn) fn = (const void*)k_fwd_x;
@@ -1229,8 +1247,19 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
     aa.ncol = n_img * C;
     aa.maps = maps;
     aa.C = C;
-    aa.cc = coils_per_cta(C);
-    aa.rows = std::max(1, 16 / aa.cc);
+    bool ct = false;
+#define TR_IS_CT(LV) case LV: ct = true; break;
+    switch (OSX) { TR_CT_LENGTHS(TR_IS_CT) default: break; }
+#undef TR_IS_CT
+    const int Wct = ct_width(OSX);
+    const bool pow2C = (C & (C - 1)) == 0;
+    if (ct && (C >= Wct || pow2C)) {
+        aa.cc = C >= Wct ? Wct : C;
+        aa.rows = Wct / aa.cc;
+    } else {
+        aa.cc = coils_per_cta(C);
+        aa.rows = std::max(1, 16 / aa.cc);
+    }
     aa.Z = Z;
     aa.Y = Y;
     aa.X = X;
@@ -1250,15 +1279,17 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
     const size_t smem = fft_smem_bytes(OSX, W) + (size_t)aa.rows * X * sizeof(float2);
     dim3 grid((unsigned)((Z * Y + aa.rows - 1) / aa.rows), (unsigned)n_img);
     const void* fn = nullptr;
-    const bool pow2 = (W == 16) && (aa.cc == 16 || aa.cc == 8 || aa.cc == 4 || aa.cc == 2 || aa.cc == 1);
-#define TR_ADJX_CASE(LV)                                                                        \
-    case LV:                                                                                    \
-        if (pow2) fn = aa.cc == 16 ? (const void*)k_adj_x_st<LV, 16>                            \
-                     : aa.cc == 8 ? (const void*)k_adj_x_st<LV, 8>                              \
-                     : aa.cc == 4 ? (const void*)k_adj_x_st<LV, 4>                              \
-                     : aa.cc == 2 ? (const void*)k_adj_x_st<LV, 2> : (const void*)k_adj_x_st<LV, 1>; \
-        else fn = (W == 12 ? (const void*)k_adj_x_ct<LV, 12> : nullptr);                        \
-        break;
+    const bool staged = ct && W == Wct;   // cc is a power of two here
+#define TR_ADJX_CASE(LV)                                                                              \
+    case LV: {                                                                                        \
+        constexpr int WV = ct_width(LV);                                                              \
+        if (staged) fn = aa.cc == 16 ? (const void*)k_adj_x_st<LV, WV, (WV >= 16 ? 16 : WV)>          \
+                       : aa.cc == 8 ? (const void*)k_adj_x_st<LV, WV, 8>                              \
+                       : aa.cc == 4 ? (const void*)k_adj_x_st<LV, WV, 4>                              \
+                       : aa.cc == 2 ? (const void*)k_adj_x_st<LV, WV, 2> : (const void*)k_adj_x_st<LV, WV, 1>; \
+        else if (W == 12 && WV == 16) fn = (const void*)k_adj_x_ct<LV, 12>;                          \
+        break;                                                                                        \
+    }
     switch (OSX) { TR_CT_LENGTHS(TR_ADJX_CASE) default: break; }
 #undef TR_ADJX_CASE
     if (!fn) fn = (const void*)k_adj_x;

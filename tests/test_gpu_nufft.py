@@ -31,7 +31,8 @@ def _coords(shape, M, rng, edge=True):
 
 # (12,16,20) .. (48,40,12) run the generic runtime-radix FFT kernels; (48,64,96)
 # and (112,128,64) have oversampled lengths with compile-time kernels.
-SHAPES = [(12, 16, 20), (16, 20, 24), (28, 24, 20), (20, 32, 36), (48, 40, 12), (48, 64, 96), (112, 128, 64)]
+SHAPES = [(12, 16, 20), (16, 20, 24), (28, 24, 20), (20, 32, 36), (48, 40, 12), (48, 64, 96), (112, 128, 64),
+          (32, 48, 256)]
 
 
 @pytest.mark.parametrize("shape", SHAPES)
@@ -111,7 +112,9 @@ def test_adjoint_is_bitwise_deterministic():
 @pytest.mark.parametrize("shape,E,C", [((12, 16, 20), 1, 1), ((12, 16, 20), 2, 3), ((12, 16, 20), 3, 16),
                                        ((12, 16, 20), 6, 16), ((48, 64, 64), 2, 16), ((48, 64, 64), 2, 12),
                                        ((48, 64, 64), 3, 6), ((48, 64, 64), 1, 40), ((48, 64, 64), 2, 8),
-                                       ((48, 64, 64), 3, 4), ((48, 64, 64), 1, 1), ((50, 64, 64), 2, 16)])
+                                       ((48, 64, 64), 3, 4), ((48, 64, 64), 1, 1), ((50, 64, 64), 2, 16),
+                                       ((32, 48, 256), 2, 16), ((32, 48, 256), 1, 12), ((32, 48, 256), 2, 4),
+                                       ((32, 48, 256), 1, 2)])
 def test_batched_coil_echo_path(shape, E, C):
     torch = _torch()
     nb = pkg("nufft_backend")
