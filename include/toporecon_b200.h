@@ -169,6 +169,22 @@ tr_status tr_power_iteration(tr_plan* plan, int32_t n_iter, void* work_images, d
  * Replaces the reference's wall-clock timers (tvme.py:509, :561-567). */
 tr_status tr_profile_nufft(tr_plan* plan, int32_t bin, int32_t reps, double* ms, double* bytes, void* stream);
 
+/* 3x3x3 convolutions of the learned PDHG warm start (no counterpart in the
+ * reference, which always starts PDHG from zeros: tvme.py:190-205).  BF16
+ * tensor-core operands, FP32 accumulation; stride 1, zero padding 1.
+ * Activations channels-last (N, D, H, W, C) bf16, weights (Cout, 27, Cin)
+ * bf16 (tap = (dz+1)*9 + (dy+1)*3 + (dx+1)); Cin even, Cout % 8 == 0, <= 128.
+ *   forward:     y (N, D, H, W, Cout) f32 = conv(x, w) + bias (bias may be NULL)
+ *   weight grad: dw (Cout, 27, Cin) f32 = sum_v gy[v, co] x[v + tap, ci]
+ *                (deterministic; needs tr_conv3d_wgrad_workspace bytes of scratch)
+ * The data gradient is tr_conv3d_fwd with the flipped, channel-swapped weights. */
+tr_status tr_conv3d_fwd(const void* x, const void* w, const float* bias, float* y, int32_t N, int32_t D,
+                        int32_t H, int32_t W, int32_t Cin, int32_t Cout, void* stream);
+tr_status tr_conv3d_wgrad_workspace(int32_t N, int32_t D, int32_t H, int32_t W, int32_t Cin, int32_t Cout,
+                                    size_t* bytes);
+tr_status tr_conv3d_wgrad(const void* x, const void* gy, float* dw, int32_t N, int32_t D, int32_t H, int32_t W,
+                          int32_t Cin, int32_t Cout, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Allocation-free stopping-tolerance sums (no counterpart in the reference).
  * For callers that cannot allocate device memory where they run the stopping
  * test -- work enqueued while a stream is captured into a CUDA graph, or hosts

@@ -28,7 +28,8 @@ EXPORTED = (
     "tr_plan_create", "tr_plan_destroy", "tr_plan_info", "tr_last_error_string", "tr_plan_set_maps",
     "tr_plan_sort_kspace", "tr_plan_unsort_kspace", "tr_nufft_forward", "tr_nufft_adjoint",
     "tr_nufft_forward_bin", "tr_nufft_adjoint_bin", "tr_plan_bin_offset", "tr_pdhg_run",
-    "tr_power_iteration", "tr_profile_nufft", "tr_tolerance_sums_noalloc",
+    "tr_power_iteration", "tr_profile_nufft", "tr_tolerance_sums_noalloc", "tr_conv3d_fwd",
+    "tr_conv3d_wgrad_workspace", "tr_conv3d_wgrad",
 )
 
 
@@ -125,6 +126,9 @@ def load() -> ctypes.CDLL:
             "tr_profile_nufft": ([vp, i32, i32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                   vp], i32),
             "tr_tolerance_sums_noalloc": ([vp, vp, i64, i32, vp, vp], i32),
+            "tr_conv3d_fwd": ([vp, vp, vp, vp, i32, i32, i32, i32, i32, i32, vp], i32),
+            "tr_conv3d_wgrad_workspace": ([i32, i32, i32, i32, i32, i32, ctypes.POINTER(ctypes.c_size_t)], i32),
+            "tr_conv3d_wgrad": ([vp, vp, vp, i32, i32, i32, i32, i32, i32, vp, ctypes.c_size_t, vp], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(lib, name)

@@ -117,6 +117,18 @@ class PdhgSolver:
         pr.use_graph = int(self.use_graph)
         return pr
 
+    def adjoint_image(self):
+        """Density-compensated, coil-combined adjoint sum_c S_c^H F_b^H (w y) per (bin, echo)."""
+        torch = self.torch
+        out = torch.empty((self.B, self.E) + self.img_shape, dtype=torch.complex64, device=self.device)
+        self.stream.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(self.stream):
+            for b in range(self.B):
+                off, cnt = self.backend.bin_offset(b), self.backend.bin_count(b)
+                self.backend.adjoint_bin(self.y[off:off + cnt], b, use_dcf=True, out=out[b])
+        torch.cuda.current_stream(self.device).wait_stream(self.stream)
+        return out
+
     # ------------------------------------------------------------------ iterate
     def iterate(self, n_iter: int, tol: float = 0.0, sigma: float | None = None, tau: float | None = None):
         """Run up to n_iter iterations from the current state; returns (iters, tols)."""
