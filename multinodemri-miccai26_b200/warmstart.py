@@ -74,6 +74,19 @@ def _flip_swap(w):
     return w.flip(1).permute(2, 1, 0).contiguous()
 
 
+def conv3d_dgrad_bf16(gy_bf, w_bf):
+    """Gradient w.r.t. the input: the forward kernel on the flipped, channel-swapped
+    weights, with their output channels padded to a multiple of 8."""
+    import torch
+    wt = _flip_swap(w_bf)
+    cin = wt.shape[0]
+    pad = (-cin) % 8
+    if pad:
+        wt = torch.cat([wt, wt.new_zeros((pad,) + tuple(wt.shape[1:]))], dim=0)
+    gx = conv3d_fwd_bf16(gy_bf, wt)
+    return gx[..., :cin].contiguous() if pad else gx
+
+
 def _make_conv_fn():
     import torch
 
@@ -89,7 +102,7 @@ def _make_conv_fn():
         def backward(ctx, gy):
             xb, wb = ctx.saved_tensors
             gb = gy.contiguous().to(torch.bfloat16)
-            gx = conv3d_fwd_bf16(gb, _flip_swap(wb)) if ctx.needs_input_grad[0] else None
+            gx = conv3d_dgrad_bf16(gb, wb) if ctx.needs_input_grad[0] else None
             gw = conv3d_wgrad_bf16(xb, gb) if ctx.needs_input_grad[1] else None
             gbias = gy.sum(dim=(0, 1, 2, 3)) if ctx.needs_input_grad[2] else None
             return gx, gw, gbias
@@ -354,7 +367,7 @@ def relative_error(net, x0, target, device="cuda", limit: int = 8) -> float:
 def main(argv=None):
     """Train the warm-start network on b200 PDHG solutions of seeded phantoms.
 
-        python multinodemri-miccai26_b200/warmstart.py --phantoms 16 --steps 600 --out warmstart_net.pt
+        python -m multinodemri-miccai26_b200.warmstart --phantoms 16 --steps 600 --out warmstart_net.pt
     """
     import argparse
     import json
@@ -393,8 +406,4 @@ def main(argv=None):
 
 
 if __name__ == "__main__":
-    import importlib
-    import sys
-    _here = Path(__file__).resolve().parent
-    sys.path.insert(0, str(_here.parent))
-    importlib.import_module(_here.name + ".warmstart").main()
+    main()

@@ -5,7 +5,7 @@ import numpy as np
 from _fixtures import pkg
 
 
-def write_dataset(root, shape=(16, 20, 18), C=3, E=2, B=3, TR=60, RO=24, seed=7, voxel=(1.5, 1.2, 1.0)):
+def write_dataset(root, shape=(16, 20, 24), C=3, E=2, B=3, TR=60, RO=24, seed=7, voxel=(1.5, 1.2, 1.0)):
     syn = pkg("synthetic")
     cfl = pkg("cfl")
     from oracle import nufft as onf

@@ -18,7 +18,7 @@ def test_reconstruct_cli_matches_oracle(tmp_path, alg):
     import torch
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
-    write_dataset(tmp_path, shape=(24, 24, 22) if alg == "tvmw" else (16, 20, 18))
+    write_dataset(tmp_path, shape=(24, 24, 22) if alg == "tvmw" else (16, 20, 24))
     cli = pkg("cli")
     out = tmp_path / "out"
     rc = cli.main(["reconstruct", "--algorithm", alg, "--", "--frac", "1.0", "--num-bins", "3", "--max-iter", "3",
