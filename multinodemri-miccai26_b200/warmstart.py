@@ -347,7 +347,7 @@ def train(x0, target, steps: int = 400, crop=(32, 32, 32), batch: int = 4, lr: f
         loss.backward()
         opt.step()
         if it % log_every == 0 or it == steps - 1:
-            history.append((it, float(loss)))
+            history.append((it, float(loss.detach())))
     return net, {"history": history, "seconds": time.perf_counter() - t0}
 
 
@@ -381,7 +381,7 @@ def main(argv=None):
     ap.add_argument("--crop", type=int, nargs=3, default=[32, 32, 32])
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--lr", type=float, default=2e-3)
-    ap.add_argument("--widths", type=int, nargs="+", default=[8, 16, 32])
+    ap.add_argument("--widths", type=int, nargs="+", default=[16, 32, 64])
     ap.add_argument("--max-iter", type=int, default=300)
     ap.add_argument("--out", default=str(WEIGHTS))
     args = ap.parse_args(argv)
@@ -401,6 +401,24 @@ def main(argv=None):
             "params": count_params(net), "pairs_seconds": t_pairs, "train_seconds": info["seconds"],
             "rel_err_train": err_train, "rel_err_holdout": err_hold, "rel_err_holdout_scaled_adjoint": base_hold,
             "loss_history": info["history"], "target": f"plain b200 PDHG, max_iter {args.max_iter}, tol {cfg.tol}"}
+    # warm-started vs plain solve on a held-out phantom
+    from dataclasses import replace
+    from .solver import PdhgSolver
+    hcfg = replace(cfg, seed=1000 + args.phantoms + args.holdout + 7)
+    ds = syn.make_geometry(hcfg)
+    syn.simulate_kspace_b200(ds, 0)
+    s = PdhgSolver(hcfg.algorithm, hcfg.img_shape, [ds.coord[ds.bin_indices(b)] for b in range(hcfg.n_bins)],
+                   ds.bin_dcf(), ds.mps, ds.bin_ksp(), l2_coupling=hcfg.l2_coupling, lam_m=hcfg.lam, lam_e=hcfg.lam)
+    plain = s.run(max_iter=args.max_iter, tol=hcfg.tol)
+    plain_img = plain.image.clone()
+    net.eval()
+    warm = warm_solve(s, hcfg, max_iter=args.max_iter, tol=hcfg.tol, model=net)
+    meta["holdout_solve"] = {
+        "plain_iterations": plain.iterations, "plain_seconds": plain.seconds,
+        "warm_iterations": warm.iterations, "warm_seconds": warm.seconds,
+        "warm_inference_seconds": warm.inference_seconds,
+        "rel_l2_warm_vs_plain": float((warm.image - plain_img).norm() / plain_img.norm())}
+    s.close()
     save_model(net, Path(args.out), meta)
     print(json.dumps(meta))
 
