@@ -129,6 +129,20 @@ class PdhgSolver:
         torch.cuda.current_stream(self.device).wait_stream(self.stream)
         return out
 
+    def data_residual(self, u):
+        """A u - y per bin in the internal k-space layout: the data dual's fixed point
+        ((q + sigma r) / (1 + sigma) = q  <=>  q = r)."""
+        torch = self.torch
+        r = torch.empty_like(self.y)
+        self.stream.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(self.stream):
+            for b in range(self.B):
+                off, cnt = self.backend.bin_offset(b), self.backend.bin_count(b)
+                self.backend.forward_bin(u[b], b, out=r[off:off + cnt])
+            r.sub_(self.y)
+        torch.cuda.current_stream(self.device).wait_stream(self.stream)
+        return r
+
     # ------------------------------------------------------------------ iterate
     def iterate(self, n_iter: int, tol: float = 0.0, sigma: float | None = None, tau: float | None = None):
         """Run up to n_iter iterations from the current state; returns (iters, tols)."""

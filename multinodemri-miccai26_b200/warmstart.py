@@ -277,8 +277,9 @@ def load_model(path: Path = WEIGHTS, device="cuda"):
 
 
 def warm_solve(solver, cfg=None, max_iter: int = 300, tol: float = 1e-3, model=None):
-    """Warm-started PDHG: u = u_bar = net(x0); returns the solver's SolveResult with
-    ``seconds`` covering the network inference and the iterations (CUDA events)."""
+    """Warm-started PDHG: u = u_bar = net(x0) and the data dual at its fixed-point
+    relation q = A u - y; returns the solver's SolveResult with ``seconds`` covering
+    the network inference, the dual set-up and the iterations (CUDA events)."""
     import torch
     net = model if model is not None else load_model(device=solver.device)
     start = torch.cuda.Event(enable_timing=True)
@@ -286,8 +287,9 @@ def warm_solve(solver, cfg=None, max_iter: int = 300, tol: float = 1e-3, model=N
     start.record()
     x0 = solver.adjoint_image()
     u0 = predict(net, x0)
+    q0 = solver.data_residual(u0)          # data dual consistent with u0
     mid.record()
-    res = solver.run(max_iter=max_iter, tol=tol, init={"u": u0, "u_bar": u0})
+    res = solver.run(max_iter=max_iter, tol=tol, init={"u": u0, "u_bar": u0, "q": q0})
     mid.synchronize()
     res.seconds += start.elapsed_time(mid) / 1e3
     res.inference_seconds = start.elapsed_time(mid) / 1e3

@@ -126,7 +126,7 @@ def test_network_gradients_bf16_precision_bound():
     l_g, l_c, g_gpu, g_cpu = _network_grads(round_bf16=False)
     assert abs(l_g - l_c) <= 3e-2 * abs(l_c)
     cos, rel = _compare(g_gpu, g_cpu)
-    assert cos > 0.97 and rel < 0.25, (cos, rel)
+    assert cos > 0.95 and rel < 0.35, (cos, rel)
 
 
 def test_training_reduces_loss():
