@@ -365,15 +365,52 @@ def relative_error(net, x0, target, device="cuda", limit: int = 8) -> float:
     return float(np.mean(errs))
 
 
+# ---------------------------------------------------------------------- evaluation
+def holdout_eval(net, cfg, seed: int, max_iter: int = 300, tol: float = 1e-3, ref_iter: int = 0, device=0) -> dict:
+    """Plain and warm-started solves of one unseen phantom to (tol, max_iter).
+
+    With ref_iter > 0 a zero-start solve of ref_iter iterations (no stopping
+    rule) stands in for the PDHG fixed point, and both results report their
+    relative L2 distance to it."""
+    from dataclasses import replace
+    from . import synthetic as syn
+    from .solver import PdhgSolver
+    hcfg = replace(cfg, seed=seed)
+    ds = syn.make_geometry(hcfg)
+    syn.simulate_kspace_b200(ds, device)
+    s = PdhgSolver(hcfg.algorithm, hcfg.img_shape, [ds.coord[ds.bin_indices(b)] for b in range(hcfg.n_bins)],
+                   ds.bin_dcf(), ds.mps, ds.bin_ksp(), l2_coupling=hcfg.l2_coupling, lam_m=hcfg.lam,
+                   lam_e=hcfg.lam, lam_w1=hcfg.lam, lam_w2=hcfg.lam, device=device)
+    rel = lambda a, b: float((a - b).norm() / b.norm().clamp_min(1e-30))
+    plain = s.run(max_iter=max_iter, tol=tol)
+    plain_img = plain.image.clone()
+    net.eval()
+    warm = warm_solve(s, hcfg, max_iter=max_iter, tol=tol, model=net)
+    out = {"workload": hcfg.name, "seed": seed, "plain_iterations": plain.iterations,
+           "plain_seconds": plain.seconds, "plain_final_tol": plain.tols[-1] if plain.tols else None,
+           "warm_iterations": warm.iterations, "warm_seconds": warm.seconds,
+           "warm_final_tol": warm.tols[-1] if warm.tols else None,
+           "warm_inference_seconds": warm.inference_seconds,
+           "rel_l2_warm_vs_plain": rel(warm.image, plain_img)}
+    if ref_iter > 0:
+        warm_img = warm.image.clone()
+        ref = s.run(max_iter=ref_iter, tol=0.0)
+        out["ref_iterations"] = ref.iterations
+        out["rel_l2_plain_vs_ref"] = rel(plain_img, ref.image)
+        out["rel_l2_warm_vs_ref"] = rel(warm_img, ref.image)
+    s.close()
+    return out
+
+
 # ---------------------------------------------------------------------- command line
 def main(argv=None):
     """Train the warm-start network on b200 PDHG solutions of seeded phantoms.
 
         python -m multinodemri-miccai26_b200.warmstart --phantoms 16 --steps 600 --out warmstart_net.pt
+        python -m multinodemri-miccai26_b200.warmstart --eval --out warmstart_net.pt --ref-iter 1500
     """
     import argparse
     import json
-    import torch
     from . import synthetic as syn
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", default="warm-96")
@@ -384,12 +421,26 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--widths", type=int, nargs="+", default=[16, 32, 64])
-    ap.add_argument("--max-iter", type=int, default=300)
+    ap.add_argument("--max-iter", type=int, default=300, help="iteration cap of the evaluated solves")
+    ap.add_argument("--target-iter", type=int, default=300,
+                    help="iterations of the zero-start solves that make the training targets")
+    ap.add_argument("--target-tol", type=float, default=None, help="stopping tolerance of the target solves")
+    ap.add_argument("--ref-iter", type=int, default=0, help="iterations of the fixed-point stand-in (0: none)")
+    ap.add_argument("--eval", action="store_true", help="evaluate the network at --out; no training")
+    ap.add_argument("--eval-config", default=None, help="workload of the held-out solve (default --config)")
     ap.add_argument("--out", default=str(WEIGHTS))
     args = ap.parse_args(argv)
     cfg = syn.CONFIGS[args.config]
+    ecfg = syn.CONFIGS[args.eval_config or args.config]
+    seed_eval = 1000 + args.phantoms + args.holdout + 7
+    if args.eval:
+        net = load_model(Path(args.out))
+        res = holdout_eval(net, ecfg, seed_eval, max_iter=args.max_iter, tol=ecfg.tol, ref_iter=args.ref_iter)
+        print(json.dumps({"eval": res, "trained": {k: v for k, v in net.meta.items() if k != "loss_history"}}))
+        return
+    t_tol = cfg.tol if args.target_tol is None else args.target_tol
     t0 = time.perf_counter()
-    x0, tgt = make_pairs(args.phantoms + args.holdout, cfg, max_iter=args.max_iter, tol=cfg.tol)
+    x0, tgt = make_pairs(args.phantoms + args.holdout, cfg, max_iter=args.target_iter, tol=t_tol)
     t_pairs = time.perf_counter() - t0
     n_train = args.phantoms * cfg.n_bins * cfg.n_echoes
     net_cfg = NetConfig(widths=tuple(args.widths), levels=len(args.widths))
@@ -402,25 +453,10 @@ def main(argv=None):
     meta = {"config": cfg.name, "phantoms": args.phantoms, "holdout": args.holdout, "steps": args.steps,
             "params": count_params(net), "pairs_seconds": t_pairs, "train_seconds": info["seconds"],
             "rel_err_train": err_train, "rel_err_holdout": err_hold, "rel_err_holdout_scaled_adjoint": base_hold,
-            "loss_history": info["history"], "target": f"plain b200 PDHG, max_iter {args.max_iter}, tol {cfg.tol}"}
-    # warm-started vs plain solve on a held-out phantom
-    from dataclasses import replace
-    from .solver import PdhgSolver
-    hcfg = replace(cfg, seed=1000 + args.phantoms + args.holdout + 7)
-    ds = syn.make_geometry(hcfg)
-    syn.simulate_kspace_b200(ds, 0)
-    s = PdhgSolver(hcfg.algorithm, hcfg.img_shape, [ds.coord[ds.bin_indices(b)] for b in range(hcfg.n_bins)],
-                   ds.bin_dcf(), ds.mps, ds.bin_ksp(), l2_coupling=hcfg.l2_coupling, lam_m=hcfg.lam, lam_e=hcfg.lam)
-    plain = s.run(max_iter=args.max_iter, tol=hcfg.tol)
-    plain_img = plain.image.clone()
-    net.eval()
-    warm = warm_solve(s, hcfg, max_iter=args.max_iter, tol=hcfg.tol, model=net)
-    meta["holdout_solve"] = {
-        "plain_iterations": plain.iterations, "plain_seconds": plain.seconds,
-        "warm_iterations": warm.iterations, "warm_seconds": warm.seconds,
-        "warm_inference_seconds": warm.inference_seconds,
-        "rel_l2_warm_vs_plain": float((warm.image - plain_img).norm() / plain_img.norm())}
-    s.close()
+            "loss_history": info["history"],
+            "target": f"zero-start b200 PDHG, max_iter {args.target_iter}, tol {t_tol}"}
+    meta["holdout_solve"] = holdout_eval(net, ecfg, seed_eval, max_iter=args.max_iter, tol=ecfg.tol,
+                                         ref_iter=args.ref_iter)
     save_model(net, Path(args.out), meta)
     print(json.dumps(meta))
 
