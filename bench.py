@@ -11,8 +11,10 @@ echo and coil).  W warm-up steps, then K steps timed with CUDA events on the
 solver's stream; then a full plain (zero-start) solve to tolerance and, when a
 trained network is present, a warm-started solve, each timed with CUDA events.
 
-The JSON line's ``value`` is the time-to-tolerance in seconds (warm-started
-when available, else plain); inputs are resident in HBM when timing starts.
+The JSON line's ``value`` is the time-to-tolerance in seconds: the
+warm-started solve when a trained network exists and its result is within
+1e-3 relative L2 of the plain result, else the plain solve (``value_source``
+says which); inputs are resident in HBM when timing starts.
 ``e2e`` is the same solve through the public API from pinned host buffers
 (plan creation, H2D of k-space and maps, sort, solve, D2H of the image).
 ``roofline`` reports the dominant NUFFT kernel (CUDA-event time of one launch
@@ -49,6 +51,7 @@ if str(REPO) not in sys.path:
 PKG = "multinodemri-miccai26_b200"
 METRIC = "TVME time-to-tol 1e-3 (s) on 1 B200, warm-start vs plain PDHG; NUFFT GB/s"
 FALLBACK_HBM_GBS = 6650.0
+WARM_MATCH = 1e-3      # warm-started result must match the plain result to this relative L2
 
 # Iterations to --tol of plain PDHG on each seeded workload, measured with the
 # b200 arm on the same seeded problem; the CPU reference arm cannot run a full
@@ -281,8 +284,10 @@ def run_b200(args):
         rel_warm = float(torch.linalg.vector_norm(a - plain_img.reshape(-1)) /
                          torch.linalg.vector_norm(plain_img.reshape(-1)))
 
-    value = warm.seconds if warm is not None else t_plain
-    value = max_over_ranks(value, world, device)
+    # the warm-started time counts only when its answer is the plain PDHG answer
+    # (relative L2 within WARM_MATCH); otherwise the plain time is the value
+    use_warm = warm is not None and rel_warm is not None and rel_warm <= WARM_MATCH
+    value = max_over_ranks(warm.seconds if use_warm else t_plain, world, device)
 
     # ---- e2e through the public API from pinned host buffers
     e2e = None
@@ -301,7 +306,7 @@ def run_b200(args):
         s2 = solver_mod.PdhgSolver(cfg.algorithm, cfg.img_shape, coords, dcfs, mps_h, ksp_h,
                                    l2_coupling=cfg.l2_coupling, lam_m=lam, lam_e=lam, lam_w1=lam, lam_w2=lam,
                                    use_graph=not args.no_graph, device=local)
-        if warm is not None:
+        if use_warm:
             r2 = ws.warm_solve(s2, cfg, max_iter=cfg.max_iter, tol=cfg.tol)
         else:
             r2 = s2.run(max_iter=cfg.max_iter, tol=cfg.tol)
@@ -339,6 +344,7 @@ def run_b200(args):
                        "coils": C, "echoes": E, "bins": B, "cones": cfg.n_interleaves, "readout": cfg.n_readout,
                        "tol": cfg.tol, "max_iter": cfg.max_iter, "l2_flush": "inputs larger than L2",
                        "parallelism": "replicas" if world > 1 else "single-gpu"},
+            "value_source": "warm-started PDHG" if use_warm else "plain PDHG",
             "time_to_tol_plain_s": round(t_plain, 4),
             "iterations_plain": r_plain.iterations,
             "tol_trace_plain": [round(t, 6) for t in r_plain.tols[::max(1, len(r_plain.tols) // 12)]],

@@ -69,6 +69,7 @@ typedef struct {
 } tr_plan_desc;
 
 #define TR_PLAN_AUTOTUNE 1       /* time candidate launch shapes at plan creation */
+#define TR_PLAN_NO_TMA 2         /* stage FFT tiles with cp.async instead of TMA (comparison runs) */
 
 typedef struct {
     int32_t os_shape[3];         /* oversampled grid (ceil(1.25 n) per axis) */

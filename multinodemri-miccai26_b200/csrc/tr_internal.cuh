@@ -30,6 +30,12 @@ tr_status cuda_fail(cudaError_t err, const char* what, const char* file, int lin
         if (_s != TR_OK) return _s;                                     \
     } while (0)
 
+// ------------------------------------------------------------------ device error word
+// Kernels that wait on hardware (mbarrier polls) give up after kMbarPollLimit
+// polls and set a bit here; the host reads it with the tolerance scalars.
+constexpr int kMbarPollLimit = 1 << 20;
+constexpr int kDevErrTmaWait = 1;
+
 // ------------------------------------------------------------------ complex helpers
 __host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -77,6 +83,13 @@ inline FftStages stages_of(const FftAxis& a) {
 struct Bin {
     int64_t offset = 0;   // first sample of the bin in the concatenated arrays
     int64_t count = 0;
+    int64_t list_offset = 0;   // first gather-list entry of the bin
+    int64_t list_count = 0;
+    int64_t n_busy = 0;        // grid tiles with at least one gather-list entry
+    int64_t work_offset = 0;   // first gridding work item of the bin
+    int64_t n_work = 0;        // work items: busy tiles, the heaviest split into list ranges
+    int64_t split_offset = 0;  // first split-tile record of the bin
+    int64_t n_split = 0;       // tiles whose list is split over several work items
 };
 
 struct PdhgGraph;        // defined in tr_pdhg.cu
@@ -100,8 +113,11 @@ struct tr_plan {
     float4* ks = nullptr;        // (kz, ky, kx, dcf) in oversampled-grid units, sorted
     void* taps = nullptr;        // per-sample first taps and KB weights (TapRec), sorted
     int32_t* perm = nullptr;     // sorted position -> acquisition index within the bin
-    int32_t* tile_start = nullptr;  // per bin [ntiles + 1] (relative to the bin offset)
-    int32_t* tile_order = nullptr;  // per bin [ntiles]: heaviest tiles first
+    int2* glist = nullptr;          // gridding gather lists: (sample in bin, packed tap offsets), all bins
+    int32_t* list_start = nullptr;  // per bin [ntiles + 1] (relative to the bin's first entry)
+    int32_t* tile_order = nullptr;  // per bin [ntiles]: busy tiles heaviest first, then empty tiles
+    int4* work = nullptr;           // gridding work items (tile, first entry, end entry, partial slot or -1)
+    int4* splits = nullptr;         // split tiles (tile, first partial slot, partial count, 0)
     int ntile[3] = {0, 0, 0};
     int64_t ntiles = 0;
     bool has_dcf = false;
@@ -120,8 +136,11 @@ struct tr_plan {
     int npartials = 0;
     double* tol_dev = nullptr;   // [4]
     double* tol_host = nullptr;  // pinned [4]
+    int* dev_err = nullptr;      // device error word (kDevErr* bits)
+    int* err_host = nullptr;     // pinned copy, refreshed with the tolerance scalars
     // launch shapes
     int line_width = 16;
+    bool use_tma = true;         // TMA-tiled FFT passes where the geometry allows
     // TVMW
     tr::WaveletPlan* wav = nullptr;
     // CUDA graph of one PDHG iteration

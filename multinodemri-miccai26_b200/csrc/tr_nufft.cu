@@ -18,6 +18,8 @@
 // The trajectory of each bin is sorted by 4x4x4 grid tile (stable counting
 // sort on the host, so the gather order and hence every sum is deterministic).
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -117,8 +119,8 @@ __global__ void __launch_bounds__(256) k_fwd_x(FwdXArgs a) {
     float2* smA = sm;
     float2* smB = sm + L * W;
     float2* tws = sm + 2 * L * W;
-    const int row0 = blockIdx.x * a.rows;
-    const int img = blockIdx.y;
+    const int img = (int)(blockIdx.x % (unsigned)a.n_img);      // images of one row block run side by side
+    const int row0 = (int)(blockIdx.x / (unsigned)a.n_img) * a.rows;
     const int c0 = blockIdx.z * a.cc;
     const int nrows = a.Z * a.Y;
     const float2* __restrict__ src = a.img + (int64_t)img * a.img_stride;
@@ -170,6 +172,8 @@ struct LineArgs {
     bool inv;
     const float2* tw;
     FftStages S;
+    int* err;               // device error word (kDevErr* bits)
+    int kA, kB;             // TMA variant: first transform row of each output box
 };
 
 // The CTA's [L][W] tile is staged with cp.async (every load in flight at
@@ -242,6 +246,7 @@ struct AdjXArgs {
     int ncol;
     const float2* maps;     // (Z, Y, X, C) or null
     int C, cc, rows;
+    int n_img;
     int Z, Y, X, OSX, h, pad;
     const float* apz;
     const float* apy;
@@ -264,8 +269,8 @@ __global__ void __launch_bounds__(256) k_adj_x(AdjXArgs a) {
     float2* acc = tws + L;                  // [rows][X]
     for (int i = threadIdx.x; i < L; i += blockDim.x) tws[i] = a.tw[i];
     for (int i = threadIdx.x; i < a.rows * a.X; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
-    const int row0 = blockIdx.x * a.rows;
-    const int img = blockIdx.y;
+    const int img = (int)(blockIdx.x % (unsigned)a.n_img);      // images of one row block run side by side
+    const int row0 = (int)(blockIdx.x / (unsigned)a.n_img) * a.rows;
     const int nrows = a.Z * a.Y;
     // buffer free during the last stage (the other one is its source)
     float2* ep = (a.S.nstages == 1) ? buf1 : (((a.S.nstages - 1) % 2 == 0) ? buf1 : buf0);
@@ -392,14 +397,59 @@ __global__ void __launch_bounds__(256) k_line_ct(LineArgs a) {
     fft_ct<L, W, 256, INV>(smA, smB, tws, store);
 }
 
+// TMA variant of k_line_ct: the [L][W] tile arrives as two boxes of L/2 rows
+// (the centred rotation m -> row (m + L/2) mod L - p_in splits the line in two
+// contiguous runs; rows outside [0, Lin) are zero-filled by the TMA unit), the
+// last FFT stage writes the result back into shared memory, and two boxes of
+// Lout/2 rows leave by TMA stores (rows o = (k + h - p_out) mod L < Lout).
+// One thread issues every copy; the rest of the CTA only runs the transform.
+// The load wait is bounded: on expiry the CTA sets kDevErrTmaWait and exits.
+template <int L, int W, bool INV>
+__global__ void __launch_bounds__(256) k_line_tma(LineArgs a, const __grid_constant__ CUtensorMap tin,
+                                                  const __grid_constant__ CUtensorMap tout) {
+    extern __shared__ __align__(128) unsigned char tsm_raw[];
+    __shared__ __align__(8) uint64_t bar;
+    // TMA boxes start on 128-byte boundaries (the launch adds 128 bytes of slack)
+    float2* tsm = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(tsm_raw) + 127) & ~uintptr_t(127));
+    float2* smA = tsm;
+    float2* smB = tsm + L * W;
+    float2* tws = tsm + 2 * L * W;
+    const int q0 = (int)blockIdx.x * W;
+    const int outer = (int)blockIdx.y;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(&bar, (unsigned)(L * W * sizeof(float2)));
+        tma_load_3d(smA, &tin, &bar, q0, L / 2 - a.p_in, outer);
+        tma_load_3d(smA + (L / 2) * W, &tin, &bar, q0, -a.p_in, outer);
+    }
+    for (int i = threadIdx.x; i < L; i += 256) tws[i] = a.tw[i];
+    const bool ok = mbar_wait_bounded(&bar, 0, kMbarPollLimit);
+    if (__syncthreads_or(!ok)) {          // every thread leaves together
+        if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
+        return;
+    }
+    float2* ep = fft_ct_free<L>(smA, smB);
+    auto store = [ep](int k, int w, float2 v) { ep[k * W + w] = v; };
+    fft_ct<L, W, 256, INV>(smA, smB, tws, store);
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int half = a.Lout / 2;
+        tma_store_3d(&tout, ep + a.kA * W, q0, 0, outer);
+        tma_store_3d(&tout, ep + a.kB * W, q0, half, outer);
+        tma_store_commit_and_drain();
+    }
+}
+
 template <int L, int W>
 __global__ void __launch_bounds__(256) k_fwd_x_ct(FwdXArgs a) {
     extern __shared__ float2 sm[];
     float2* smA = sm;
     float2* smB = sm + L * W;
     float2* tws = sm + 2 * L * W;
-    const int row0 = blockIdx.x * a.rows;
-    const int img = blockIdx.y;
+    const int img = (int)(blockIdx.x % (unsigned)a.n_img);      // images of one row block run side by side
+    const int row0 = (int)(blockIdx.x / (unsigned)a.n_img) * a.rows;
     const int c0 = blockIdx.z * a.cc;
     const int nrows = a.Z * a.Y;
     const int cc = a.cc;
@@ -444,8 +494,8 @@ __global__ void __launch_bounds__(256) k_adj_x_ct(AdjXArgs a) {
     float2* acc = tws + L;                  // [rows][X]
     for (int i = threadIdx.x; i < L; i += 256) tws[i] = a.tw[i];
     for (int i = threadIdx.x; i < a.rows * a.X; i += 256) acc[i] = make_float2(0.f, 0.f);
-    const int row0 = blockIdx.x * a.rows;
-    const int img = blockIdx.y;
+    const int img = (int)(blockIdx.x % (unsigned)a.n_img);      // images of one row block run side by side
+    const int row0 = (int)(blockIdx.x / (unsigned)a.n_img) * a.rows;
     const int nrows = a.Z * a.Y;
     const int cc = a.cc;
     float2* ep = fft_ct_free<L>(buf0, buf1);
@@ -520,8 +570,8 @@ __global__ void __launch_bounds__(256) k_fwd_x_st(FwdXArgs a) {
     float2* s_img = smB;                 // [ROWS][X]
     float2* s_map = smB + ROWS * X;      // [ROWS][X][CC]
     __shared__ float s_apzy[ROWS];
-    const int row0 = blockIdx.x * ROWS;
-    const int img = blockIdx.y;
+    const int img = (int)(blockIdx.x % (unsigned)a.n_img);      // images of one row block run side by side
+    const int row0 = (int)(blockIdx.x / (unsigned)a.n_img) * ROWS;
     const int c0 = blockIdx.z * CC;
     const int nrows = a.Z * a.Y;
     const float2* __restrict__ src = a.img + (int64_t)img * a.img_stride;
@@ -589,8 +639,8 @@ __global__ void __launch_bounds__(256) k_adj_x_st(AdjXArgs a) {
     float2* acc = tws + L;                  // [ROWS][X]
     for (int i = threadIdx.x; i < L; i += 256) tws[i] = a.tw[i];
     for (int i = threadIdx.x; i < ROWS * a.X; i += 256) acc[i] = make_float2(0.f, 0.f);
-    const int row0 = blockIdx.x * ROWS;
-    const int img = blockIdx.y;
+    const int img = (int)(blockIdx.x % (unsigned)a.n_img);      // images of one row block run side by side
+    const int row0 = (int)(blockIdx.x / (unsigned)a.n_img) * ROWS;
     const int nrows = a.Z * a.Y;
     const int X = a.X;
     float2* ep = fft_ct_free<L>(buf0, buf1);
@@ -774,107 +824,95 @@ __global__ void __launch_bounds__(256) k_interp(const float2* __restrict__ grid,
 // ------------------------------------------------------------------ gridding (tile gather)
 // One CTA owns a 4x4x4 tile of the oversampled grid and up to 16*CG columns.
 // Thread (row, g): row = (pz, py) of the tile (16 rows, each 4 x-points),
-// g = column group of CG consecutive columns.  Candidate samples come from
-// the home tiles that can reach the tile; 256 are tested per round and the
-// ones whose support meets the tile are compacted in candidate order (block
-// prefix sum, no atomics); their weights and weighted values are staged in
-// shared memory 64 at a time and every (point, column) accumulator sums them
-// in that fixed order.  Bitwise reproducible.
+// g = column group of CG consecutive columns.  The plan holds, per tile, the
+// list of samples whose KB support meets it (in sorted-sample order) with the
+// tap offsets of the tile origin, so a CTA only stages those samples' weights
+// and dcf-weighted values in shared memory, 64 at a time, and every
+// (point, column) accumulator sums them in list order: no atomics, bitwise
+// reproducible.  The launch runs work items first: a tile's list range
+// (lists longer than kSplitEntries are cut into ranges whose partial tiles go
+// to a scratch buffer, the first range writing the grid), heaviest first; the
+// trailing CTAs write zeros into tiles no sample reaches, kZeroTiles each.
+// k_spread_reduce then adds the partial tiles to the grid in range order.
 constexpr int kTile = 4;
-constexpr int kSpreadRound = 256;   // candidates tested per round
-constexpr int kSpreadSub = 64;      // candidates staged per sub-chunk
+constexpr int kSpreadSub = 64;      // list entries staged per sub-chunk
+constexpr int kZeroTiles = 4;       // empty tiles per zero-fill CTA
+constexpr int kSplitEntries = 256;  // longest list range of one work item
 
 struct SpreadArgs {
     const float4* ks;          // bin base (dcf in .w)
     const TapRec* taps;        // bin base
-    const int32_t* tile_start; // bin base [ntiles + 1]
-    const int32_t* tile_order; // bin base [ntiles] or null
+    const int2* list;          // bin base: (sample, packed tap offsets of the tile origin)
+    const int32_t* list_start; // bin base [ntiles + 1]
+    const int32_t* tile_order; // bin base [ntiles]: busy tiles, then empty tiles
+    const int4* work;          // bin base [n_work]: (tile, first entry, end entry, partial slot or -1)
+    int n_busy, n_empty, n_work;
+    float2* partials;          // [slot][64 points][ncol] partial tiles of split lists
     const float2* vals;        // (M_b, ncol) bin base
     int ncol, cchunk;          // columns per CTA (blockIdx.y selects the chunk)
     int use_dcf;
     float2* grid;              // (OSZ, OSY, OSX, ncol)
     int os0, os1, os2;
-    int nt0, nt1, nt2;
+    int nt1, nt2;
 };
 
-__device__ __forceinline__ int wrap_rel(int t0, int b0, int os) {
-    // (t0 - b0) mod os mapped to (-os + 4, 4]: the tap index of point t0
-    int r = pmod(t0 - b0, os);
-    if (r > 4) r -= os;
-    return r;
+// Packed tap offset of a tile origin: byte i holds (offset + 128) for axis z, y, x.
+__host__ __device__ __forceinline__ int pack_rel(int rz, int ry, int rx) {
+    return ((rz + 128) & 0xff) | (((ry + 128) & 0xff) << 8) | (((rx + 128) & 0xff) << 16);
+}
+
+__device__ __forceinline__ void tile_geometry(const SpreadArgs& a, int tile, int& t0z, int& t0y, int& t0x,
+                                              int& Tz, int& Ty, int& Tx) {
+    const int tz = tile / (a.nt1 * a.nt2);
+    const int trem = tile - tz * a.nt1 * a.nt2;
+    const int ty = trem / a.nt2;
+    const int tx = trem - ty * a.nt2;
+    t0z = tz * kTile;
+    t0y = ty * kTile;
+    t0x = tx * kTile;
+    Tz = min(kTile, a.os0 - t0z);
+    Ty = min(kTile, a.os1 - t0y);
+    Tx = min(kTile, a.os2 - t0x);
 }
 
 template <int CG>
 __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    __shared__ int run_start[64];
-    __shared__ int run_pref[65];
-    __shared__ int nlist[3];
-    __shared__ int tlist[3][4];
-    __shared__ int warp_cnt[8];
-    __shared__ int warp_off[9];
-    __shared__ int l_s[kSpreadRound];        // compacted sample indices
-    __shared__ int l_rel[kSpreadRound];      // packed tap offsets of the tile origin
+    __shared__ int l_rel[kSpreadSub];
     float* c_w = reinterpret_cast<float*>(smraw);                        // [kSpreadSub][16]
     float2* dq = reinterpret_cast<float2*>(c_w + 16 * kSpreadSub);       // [kSpreadSub][ncc]
+    const int tid = threadIdx.x;
+
+    if ((int)blockIdx.x >= a.n_work) {
+        // ---- zero fill of tiles that no sample reaches (all columns, chunk 0 only)
+        if (blockIdx.y != 0) return;
+        const int warp = tid >> 5, lane = tid & 31;
+        const int z0 = ((int)blockIdx.x - a.n_work) * kZeroTiles;
+        for (int r = warp; r < kZeroTiles * 16; r += 8) {
+            const int zi = z0 + (r >> 4);
+            if (zi >= a.n_empty) break;
+            int t0z, t0y, t0x, Tz, Ty, Tx;
+            tile_geometry(a, a.tile_order[a.n_busy + zi], t0z, t0y, t0x, Tz, Ty, Tx);
+            const int pz = (r >> 2) & 3, py = r & 3;
+            if (pz >= Tz || py >= Ty) continue;
+            float2* dst = a.grid + (((int64_t)(t0z + pz) * a.os1 + (t0y + py)) * a.os2 + t0x) * a.ncol;
+            const int n2 = Tx * a.ncol;
+            if ((reinterpret_cast<uintptr_t>(dst) & 15) == 0 && (n2 & 1) == 0) {
+                float4* d4 = reinterpret_cast<float4*>(dst);
+                for (int i = lane; i < (n2 >> 1); i += 32) d4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+                for (int i = lane; i < n2; i += 32) dst[i] = make_float2(0.f, 0.f);
+            }
+        }
+        return;
+    }
 
     const int col0 = blockIdx.y * a.cchunk;
     const int ncc = min(a.cchunk, a.ncol - col0);
-    const int tile = a.tile_order ? a.tile_order[blockIdx.x] : (int)blockIdx.x;
-    const int tz = tile / (a.nt1 * a.nt2);
-    const int trem = tile - tz * a.nt1 * a.nt2;
-    const int ty = trem / a.nt2;
-    const int tx = trem - ty * a.nt2;
-    const int t0z = tz * kTile, t0y = ty * kTile, t0x = tx * kTile;
-    const int Tz = min(kTile, a.os0 - t0z), Ty = min(kTile, a.os1 - t0y), Tx = min(kTile, a.os2 - t0x);
-    const int tid = threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5;
-
-    // home tiles that can reach this tile: per axis the distinct tiles holding
-    // floor(k) in [t0 - 2, t0 + T + 1] (wrapped); at most four per axis
-    if (tid < 3) {
-        const int t0 = tid == 0 ? t0z : (tid == 1 ? t0y : t0x);
-        const int Tn = tid == 0 ? Tz : (tid == 1 ? Ty : Tx);
-        const int osn = tid == 0 ? a.os0 : (tid == 1 ? a.os1 : a.os2);
-        int n = 0, prev = -1;
-        for (int pos = t0 - 2; pos <= t0 + Tn + 1; ++pos) {
-            const int tt = pmod(pos, osn) / kTile;
-            if (tt != prev && n < 4) {
-                bool seen = false;
-                for (int i = 0; i < n; ++i) seen |= (tlist[tid][i] == tt);
-                if (!seen) tlist[tid][n++] = tt;
-            }
-            prev = tt;
-        }
-        nlist[tid] = n;
-    }
-    __syncthreads();
-    const int nruns = nlist[0] * nlist[1] * nlist[2];
-    if (tid < nruns) {
-        const int iz = tid / (nlist[1] * nlist[2]);
-        const int iy = (tid / nlist[2]) % nlist[1];
-        const int ix = tid % nlist[2];
-        const int id = (tlist[0][iz] * a.nt1 + tlist[1][iy]) * a.nt2 + tlist[2][ix];
-        run_start[tid] = a.tile_start[id];
-        run_pref[tid + 1] = a.tile_start[id + 1] - a.tile_start[id];
-    }
-    __syncthreads();
-    if (tid < 32) {   // inclusive scan of the run lengths by one warp
-        int carry = 0;
-        for (int b0 = 0; b0 < nruns; b0 += 32) {
-            int v = (b0 + lane < nruns) ? run_pref[b0 + lane + 1] : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, v, o);
-                if (lane >= o) v += t;
-            }
-            if (b0 + lane < nruns) run_pref[b0 + lane + 1] = v + carry;
-            carry += __shfl_sync(0xffffffffu, v, 31);
-        }
-        if (lane == 0) run_pref[0] = 0;
-    }
-    __syncthreads();
-    const int total = run_pref[nruns];
+    const int4 item = a.work[blockIdx.x];
+    const int tile = item.x, beg = item.y, end = item.z, slot = item.w;
+    int t0z, t0y, t0x, Tz, Ty, Tx;
+    tile_geometry(a, tile, t0z, t0y, t0x, Tz, Ty, Tx);
 
     const int row = tid >> 4;
     const int pz = row >> 2, py = row & 3;
@@ -886,83 +924,57 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
 #pragma unroll
         for (int j = 0; j < CG; ++j) acc[x][j] = make_float2(0.f, 0.f);
 
-    for (int base = 0; base < total; base += kSpreadRound) {
-        // ---- test 256 candidates and compact the ones meeting the tile
-        int flag = 0, sidx = 0, packed = 0;
-        const int ci = base + tid;
-        if (ci < total) {
-            int lo = 0, hi = nruns - 1;          // run r with pref[r] <= ci < pref[r+1]
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (run_pref[mid] <= ci) lo = mid; else hi = mid - 1;
-            }
-            sidx = run_start[lo] + (ci - run_pref[lo]);
-            const int4 b = a.taps[sidx].b;
-            const int rz = wrap_rel(t0z, b.x, a.os0);
-            const int ry = wrap_rel(t0y, b.y, a.os1);
-            const int rx = wrap_rel(t0x, b.z, a.os2);
-            flag = (rz + Tz - 1 >= 0) && (ry + Ty - 1 >= 0) && (rx + Tx - 1 >= 0);
-            packed = ((rz + 128) & 0xff) | (((ry + 128) & 0xff) << 8) | (((rx + 128) & 0xff) << 16);
+    for (int base = beg; base < end; base += kSpreadSub) {
+        const int ns = min(kSpreadSub, end - base);
+        if (tid < 4 * ns) {
+            const int cand = tid >> 2, part = tid & 3;
+            const int2 e = a.list[base + cand];
+            reinterpret_cast<float4*>(c_w)[cand * 4 + part] = a.taps[e.x].w[part];
+            if (part == 0) l_rel[cand] = e.y;
         }
-        const unsigned bal = __ballot_sync(0xffffffffu, flag);
-        if (lane == 0) warp_cnt[warp] = __popc(bal);
-        __syncthreads();
-        if (tid == 0) {
-            warp_off[0] = 0;
-            for (int w = 0; w < 8; ++w) warp_off[w + 1] = warp_off[w] + warp_cnt[w];
+        for (int i = tid; i < ns * ncc; i += 256) {
+            const int cand = i / ncc, col = i - cand * ncc;
+            const int sm = a.list[base + cand].x;
+            float2 v = a.vals[(int64_t)sm * a.ncol + col0 + col];
+            if (a.use_dcf) v = cscale(v, a.ks[sm].w);
+            dq[i] = v;
         }
         __syncthreads();
-        const int nl = warp_off[8];
-        if (flag) {
-            const int pos = warp_off[warp] + __popc(bal & ((1u << lane) - 1u));
-            l_s[pos] = sidx;
-            l_rel[pos] = packed;
-        }
-        __syncthreads();
-        // ---- accumulate the compacted list, kSpreadSub candidates at a time
-        for (int sub = 0; sub < nl; sub += kSpreadSub) {
-            const int ns = min(kSpreadSub, nl - sub);
-            if (tid < 4 * ns) {
-                const int cand = tid >> 2, part = tid & 3;
-                reinterpret_cast<float4*>(c_w)[cand * 4 + part] = a.taps[l_s[sub + cand]].w[part];
-            }
-            for (int i = tid; i < ns * ncc; i += 256) {
-                const int cand = i / ncc, col = i - cand * ncc;
-                const int sm = l_s[sub + cand];
-                float2 v = a.vals[(int64_t)sm * a.ncol + col0 + col];
-                if (a.use_dcf) v = cscale(v, a.ks[sm].w);
-                dq[i] = v;
-            }
-            __syncthreads();
-            for (int cc = 0; cc < ns; ++cc) {
-                const int pk = l_rel[sub + cc];
-                const int az = (pk & 0xff) - 128 + pz;
-                const int ay = ((pk >> 8) & 0xff) - 128 + py;
-                if ((unsigned)az > 4u || (unsigned)ay > 4u) continue;
-                const float* w = c_w + 16 * cc;
-                const float wzy = w[az] * w[5 + ay];
-                if (wzy == 0.f) continue;
-                const int rx = ((pk >> 16) & 0xff) - 128;
-                float2 v[CG];
+        for (int cc = 0; cc < ns; ++cc) {
+            const int pk = l_rel[cc];
+            const int az = (pk & 0xff) - 128 + pz;
+            const int ay = ((pk >> 8) & 0xff) - 128 + py;
+            if ((unsigned)az > 4u || (unsigned)ay > 4u) continue;
+            const float* w = c_w + 16 * cc;
+            const float wzy = w[az] * w[5 + ay];
+            if (wzy == 0.f) continue;
+            const int rx = ((pk >> 16) & 0xff) - 128;
+            float2 v[CG];
 #pragma unroll
-                for (int j = 0; j < CG; ++j) v[j] = (c_lo + j < ncc) ? dq[cc * ncc + c_lo + j] : make_float2(0.f, 0.f);
+            for (int j = 0; j < CG; ++j) v[j] = (c_lo + j < ncc) ? dq[cc * ncc + c_lo + j] : make_float2(0.f, 0.f);
 #pragma unroll
-                for (int x = 0; x < 4; ++x) {
-                    const int ax = rx + x;
-                    if ((unsigned)ax > 4u) continue;
-                    const float wt = wzy * w[10 + ax];
+            for (int x = 0; x < 4; ++x) {
+                const int ax = rx + x;
+                if ((unsigned)ax > 4u) continue;
+                const float wt = wzy * w[10 + ax];
 #pragma unroll
-                    for (int j = 0; j < CG; ++j) {
-                        acc[x][j].x += wt * v[j].x;
-                        acc[x][j].y += wt * v[j].y;
-                    }
+                for (int j = 0; j < CG; ++j) {
+                    acc[x][j].x += wt * v[j].x;
+                    acc[x][j].y += wt * v[j].y;
                 }
             }
-            __syncthreads();
         }
+        __syncthreads();
     }
-    // ---- write the tile: each thread its 4 x-points x CG columns
-    if (pz < Tz && py < Ty) {
+    // ---- write the tile (or the partial tile of a split list): 4 x-points x CG columns
+    if (slot >= 0) {
+        float2* dst = a.partials + ((int64_t)slot * 64 + row * 4) * a.ncol + col0 + c_lo;
+#pragma unroll
+        for (int x = 0; x < 4; ++x)
+#pragma unroll
+            for (int j = 0; j < CG; ++j)
+                if (c_lo + j < ncc) dst[(int64_t)x * a.ncol + j] = acc[x][j];
+    } else if (pz < Tz && py < Ty) {
         const int64_t rowg = ((int64_t)(t0z + pz) * a.os1 + (t0y + py)) * a.os2 + t0x;
 #pragma unroll
         for (int x = 0; x < 4; ++x) {
@@ -972,6 +984,23 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
             for (int j = 0; j < CG; ++j)
                 if (c_lo + j < ncc) dst[j] = acc[x][j];
         }
+    }
+}
+
+// Split lists: grid tile += its partial tiles, in range order (one CTA per tile).
+__global__ void __launch_bounds__(256) k_spread_reduce(SpreadArgs a, const int4* __restrict__ splits) {
+    const int4 sp = splits[blockIdx.x];
+    int t0z, t0y, t0x, Tz, Ty, Tx;
+    tile_geometry(a, sp.x, t0z, t0y, t0x, Tz, Ty, Tx);
+    const int n = 64 * a.ncol;
+    for (int i = threadIdx.x; i < n; i += 256) {
+        const int pt = i / a.ncol, col = i - pt * a.ncol;
+        const int pz = pt >> 4, py = (pt >> 2) & 3, px = pt & 3;
+        if (pz >= Tz || py >= Ty || px >= Tx) continue;
+        float2* g = a.grid + (((int64_t)(t0z + pz) * a.os1 + (t0y + py)) * a.os2 + (t0x + px)) * a.ncol + col;
+        float2 v = *g;
+        for (int s = 0; s < sp.z; ++s) v = cadd(v, a.partials[((int64_t)(sp.y + s) * 64 + pt) * a.ncol + col]);
+        *g = v;
     }
 }
 
@@ -1053,6 +1082,58 @@ tr_status ensure_nufft_buffers(tr_plan* p, size_t ncol) {
     return TR_OK;
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once (no libcuda link).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+    });
+    return fn;
+}
+
+// 3-D map over complex64 data [d2][d1][d0] (8-byte elements), box [1][b1][b0].
+static bool encode_map_3d(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint32_t b0,
+                          uint32_t b1) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || ((uintptr_t)base & 15) || (d0 * 8) % 16 || b0 > 256 || b1 > 256 || b0 > d0) return false;
+    const cuuint64_t dims[3] = {d0, d1, d2};
+    const cuuint64_t strides[2] = {d0 * 8, d0 * d1 * 8};
+    const cuuint32_t box[3] = {b0, b1, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_INT64, 3, const_cast<void*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tensor maps for k_line_tma, or false when the line's geometry does not split
+// into the two-box form (odd lengths, unaligned shared-memory box starts, ...).
+static bool line_tma_setup(LineArgs& la, int L, int W, int64_t outer, CUtensorMap* tin, CUtensorMap* tout) {
+    if (L % 2 || la.Lout % 2 || la.inner % 2 || la.inner < W || la.inner >= (int64_t)INT32_MAX || outer > 65535 ||
+        L / 2 > 256 || la.Lout / 2 > 256 || la.p_in > L / 2)
+        return false;
+    const int half = la.Lout / 2;
+    auto pm = [L](int v) {
+        v %= L;
+        return v < 0 ? v + L : v;
+    };
+    const int shift = la.h - la.p_out;
+    const int kA = pm(-shift), kB = pm(half - shift);
+    if (kA + half > L || kB + half > L) return false;
+    if (((int64_t)kA * W * 8) % 128 || ((int64_t)kB * W * 8) % 128 || ((int64_t)(L / 2) * W * 8) % 128) return false;
+    if (!encode_map_3d(tin, la.in, (uint64_t)la.inner, (uint64_t)la.Lin, (uint64_t)outer, (uint32_t)W, (uint32_t)(L / 2)))
+        return false;
+    if (!encode_map_3d(tout, la.out, (uint64_t)la.inner, (uint64_t)la.Lout, (uint64_t)outer, (uint32_t)W, (uint32_t)half))
+        return false;
+    la.kA = kA;
+    la.kB = kB;
+    return true;
+}
+
 static tr_status launch_line(tr_plan* p, int axis, const float2* in, float2* out, int64_t outer, int64_t inner,
                              int Lin, int Lout, int p_in, int p_out, bool inv, cudaStream_t st) {
     const FftAxis& A = p->ax[axis];
@@ -1066,25 +1147,37 @@ static tr_status launch_line(tr_plan* p, int axis, const float2* in, float2* out
     la.p_out = p_out;
     la.h = A.h;
     la.W = p->line_width;
-    la.vec16 = ((inner % 2) == 0 && (la.W % 2) == 0 && ((uintptr_t)in % 16) == 0) ? 1 : 0;
     la.inv = inv;
     la.tw = A.twiddle;
     la.S = stages_of(A);
+    la.err = p->dev_err;
+    la.kA = la.kB = 0;
     const void* fn = nullptr;
+    CUtensorMap tin, tout;
+    bool tma = false;
 #define TR_LINE_CASE(LV)                                                                                  \
     case LV:                                                                                              \
         la.W = ct_width(LV);                                                                              \
-        fn = inv ? (const void*)k_line_ct<LV, ct_width(LV), true> : (const void*)k_line_ct<LV, ct_width(LV), false>; \
+        tma = p->use_tma && line_tma_setup(la, LV, ct_width(LV), outer, &tin, &tout);                     \
+        if (tma)                                                                                          \
+            fn = inv ? (const void*)k_line_tma<LV, ct_width(LV), true> : (const void*)k_line_tma<LV, ct_width(LV), false>; \
+        else                                                                                              \
+            fn = inv ? (const void*)k_line_ct<LV, ct_width(LV), true> : (const void*)k_line_ct<LV, ct_width(LV), false>; \
         break;
     switch (A.L) { TR_CT_LENGTHS(TR_LINE_CASE) default: break; }
 #undef TR_LINE_CASE
     if (!fn) fn = (const void*)k_line;
     la.vec16 = ((inner % 2) == 0 && (la.W % 2) == 0 && ((uintptr_t)in % 16) == 0) ? 1 : 0;
-    const size_t smem = fft_smem_bytes(A.L, la.W);
+    const size_t smem = fft_smem_bytes(A.L, la.W) + (tma ? 128 : 0);
     dim3 grid((unsigned)((inner + la.W - 1) / la.W), (unsigned)outer);
     TR_TRY(set_smem_limit(fn, smem));
-    void* args[] = {&la};
-    TR_CUDA(cudaLaunchKernel(fn, grid, dim3(256), args, smem, st));
+    if (tma) {
+        void* args[] = {&la, &tin, &tout};
+        TR_CUDA(cudaLaunchKernel(fn, grid, dim3(256), args, smem, st));
+    } else {
+        void* args[] = {&la};
+        TR_CUDA(cudaLaunchKernel(fn, grid, dim3(256), args, smem, st));
+    }
     return TR_OK;
 }
 
@@ -1130,7 +1223,8 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
     fa.ncol = n_img * C;
     const int W = fa.rows * fa.cc;
     const size_t smem = fft_smem_bytes(OSX, W);
-    dim3 grid((unsigned)((Z * Y + fa.rows - 1) / fa.rows), (unsigned)n_img, (unsigned)((C + fa.cc - 1) / fa.cc));
+    // the n_img CTAs of one row block are adjacent, so the coil-map rows they share come from L2
+    dim3 grid((unsigned)(((Z * Y + fa.rows - 1) / fa.rows) * n_img), 1u, (unsigned)((C + fa.cc - 1) / fa.cc));
     const void* fn = nullptr;
     // staged variant when a row's coil-map slice fits the free FFT buffer
     const bool staged = ct && W == Wct && fa.cc >= 4 && (size_t)fa.rows * X * (fa.cc + 1) <= (size_t)OSX * W;
@@ -1197,14 +1291,20 @@ static tr_status launch_spread_t(const SpreadArgs& sa, unsigned ntiles, unsigned
     return TR_OK;
 }
 
-// gridding: one CTA per (4x4x4 tile, chunk of <= 128 columns)
+// gridding: one CTA per (busy 4x4x4 tile, chunk of <= 128 columns), then the zero-fill CTAs
 static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, bool use_dcf, cudaStream_t st) {
     const Bin& b = p->bins[bin];
     SpreadArgs sa;
     sa.ks = p->ks + b.offset;
     sa.taps = reinterpret_cast<const TapRec*>(p->taps) + b.offset;
-    sa.tile_start = p->tile_start + (int64_t)bin * (p->ntiles + 1);
+    sa.list = p->glist + b.list_offset;
+    sa.list_start = p->list_start + (int64_t)bin * (p->ntiles + 1);
     sa.tile_order = p->tile_order + (int64_t)bin * p->ntiles;
+    sa.work = p->work + b.work_offset;
+    sa.n_busy = (int)b.n_busy;
+    sa.n_empty = (int)(p->ntiles - b.n_busy);
+    sa.n_work = (int)b.n_work;
+    sa.partials = p->bufB;     // free during gridding (the adjoint z pass fills it afterwards)
     sa.vals = ksp;
     sa.ncol = ncol;
     const int nch = (ncol + 127) / 128;
@@ -1214,16 +1314,20 @@ static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, 
     sa.os0 = p->os[0];
     sa.os1 = p->os[1];
     sa.os2 = p->os[2];
-    sa.nt0 = p->ntile[0];
     sa.nt1 = p->ntile[1];
     sa.nt2 = p->ntile[2];
     const int cg = (sa.cchunk + 15) / 16;
-    const unsigned nt = (unsigned)p->ntiles;
-    if (cg <= 1) return launch_spread_t<1>(sa, nt, nch, st);
-    if (cg <= 2) return launch_spread_t<2>(sa, nt, nch, st);
-    if (cg <= 4) return launch_spread_t<4>(sa, nt, nch, st);
-    if (cg <= 6) return launch_spread_t<6>(sa, nt, nch, st);
-    return launch_spread_t<8>(sa, nt, nch, st);
+    const unsigned nx = (unsigned)(sa.n_work + (sa.n_empty + kZeroTiles - 1) / kZeroTiles);
+    if (cg <= 1) TR_TRY(launch_spread_t<1>(sa, nx, nch, st));
+    else if (cg <= 2) TR_TRY(launch_spread_t<2>(sa, nx, nch, st));
+    else if (cg <= 4) TR_TRY(launch_spread_t<4>(sa, nx, nch, st));
+    else if (cg <= 6) TR_TRY(launch_spread_t<6>(sa, nx, nch, st));
+    else TR_TRY(launch_spread_t<8>(sa, nx, nch, st));
+    if (b.n_split > 0) {
+        k_spread_reduce<<<(unsigned)b.n_split, 256, 0, st>>>(sa, p->splits + b.split_offset);
+        TR_CHECK_LAUNCH();
+    }
+    return TR_OK;
 }
 
 // z pass (inverse, crop to Z): [1][OSZ -> Z][OSY * OSX * ncol]
@@ -1245,6 +1349,7 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
     AdjXArgs aa;
     aa.in = p->bufA;
     aa.ncol = n_img * C;
+    aa.n_img = n_img;
     aa.maps = maps;
     aa.C = C;
     bool ct = false;
@@ -1277,7 +1382,7 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
     aa.accumulate = 0;
     const int W = aa.rows * aa.cc;
     const size_t smem = fft_smem_bytes(OSX, W) + (size_t)aa.rows * X * sizeof(float2);
-    dim3 grid((unsigned)((Z * Y + aa.rows - 1) / aa.rows), (unsigned)n_img);
+    dim3 grid((unsigned)(((Z * Y + aa.rows - 1) / aa.rows) * n_img));
     const void* fn = nullptr;
     const bool staged = ct && W == Wct;   // cc is a power of two here
 #define TR_ADJX_CASE(LV)                                                                              \
@@ -1405,7 +1510,10 @@ static void plan_free(tr_plan* p) {
     cudaFree(p->ks);
     cudaFree(p->taps);
     cudaFree(p->perm);
-    cudaFree(p->tile_start);
+    cudaFree(p->glist);
+    cudaFree(p->work);
+    cudaFree(p->splits);
+    cudaFree(p->list_start);
     cudaFree(p->tile_order);
     cudaFree(p->maps);
     cudaFree(p->bufA);
@@ -1414,6 +1522,8 @@ static void plan_free(tr_plan* p) {
     cudaFree(p->one_out);
     cudaFree(p->partials);
     cudaFree(p->tol_dev);
+    cudaFree(p->dev_err);
+    if (p->err_host) cudaFreeHost(p->err_host);
     if (p->tol_host) cudaFreeHost(p->tol_host);
     cudaSetDevice(cur);
     delete p;
@@ -1429,6 +1539,115 @@ struct DeviceGuard {
         if (prev >= 0) cudaSetDevice(prev);
     }
 };
+
+// Tiles of one axis met by the KB support of coordinate k: the first tap
+// ceil(k - 2) (in double, as the device's axis_taps), four taps, and a fifth
+// where the device gives it a nonzero weight (|(b0 + 4 - k) / 2| <= 1 in float);
+// tiles in order of first appearance with the tap offset of each tile origin.
+static int axis_tiles(float k, int os, int* tile, int* rel) {
+    const int b0 = (int)std::ceil((double)k - 2.0);
+    volatile float d4 = ((float)(b0 + 4) - k) * 0.5f;
+    const int nt = std::fabs((float)d4) <= 1.0f ? 5 : 4;
+    int n = 0;
+    for (int t = 0; t < nt; ++t) {
+        int pos = (b0 + t) % os;
+        if (pos < 0) pos += os;
+        const int tt = pos / kTile;
+        bool seen = false;
+        for (int i = 0; i < n; ++i) seen |= tile[i] == tt;
+        if (seen) continue;
+        int r = (tt * kTile - b0) % os;     // tap index of the tile origin, in (-os + 4, 4]
+        if (r < 0) r += os;
+        if (r > 4) r -= os;
+        tile[n] = tt;
+        rel[n] = r;
+        ++n;
+    }
+    return n;
+}
+
+// Gather lists of one bin (ks: its tile-sorted scaled coordinates): for every
+// grid tile the samples whose support meets it, in sorted-sample order, as
+// (sample, packed tap offsets); list_start [ntiles + 1] relative to the bin's
+// first entry; order: busy tiles by entry count (heaviest first, stable),
+// then the empty tiles.
+static tr_status build_gather_lists(tr_plan* p, int bin, const float4* ks, int64_t M, std::vector<int2>& glist,
+                                    int32_t* list_start, int32_t* order, std::vector<int4>& work,
+                                    std::vector<int4>& splits) {
+    const int64_t nt = p->ntiles;
+    std::vector<int64_t> cnt((size_t)nt + 1, 0);
+    auto visit = [&](auto&& emit) {
+        for (int64_t m = 0; m < M; ++m) {
+            int tz[5], ty[5], tx[5], rz[5], ry[5], rx[5];
+            const int nz = axis_tiles(ks[m].x, p->os[0], tz, rz);
+            const int ny = axis_tiles(ks[m].y, p->os[1], ty, ry);
+            const int nx = axis_tiles(ks[m].z, p->os[2], tx, rx);
+            for (int i = 0; i < nz; ++i)
+                for (int j = 0; j < ny; ++j)
+                    for (int l = 0; l < nx; ++l)
+                        emit(((int64_t)tz[i] * p->ntile[1] + ty[j]) * p->ntile[2] + tx[l], (int32_t)m,
+                             pack_rel(rz[i], ry[j], rx[l]));
+        }
+    };
+    visit([&](int64_t t, int32_t, int) { cnt[(size_t)t + 1]++; });
+    for (int64_t t = 0; t < nt; ++t) cnt[(size_t)t + 1] += cnt[(size_t)t];
+    const int64_t total = cnt[(size_t)nt];
+    if (total > (int64_t)INT32_MAX)
+        return fail(TR_ERR_UNSUPPORTED, "gridding lists of one bin exceed 2^31 entries; split the bin");
+    Bin& B = p->bins[bin];
+    B.list_offset = (int64_t)glist.size();
+    B.list_count = total;
+    glist.resize(glist.size() + (size_t)total);
+    int2* dst = glist.data() + B.list_offset;
+    std::vector<int64_t> cur(cnt.begin(), cnt.end() - 1);
+    visit([&](int64_t t, int32_t m, int packed) { dst[cur[(size_t)t]++] = make_int2(m, packed); });
+    std::vector<std::pair<int64_t, int32_t>> busy;
+    std::vector<int32_t> empty;
+    for (int64_t t = 0; t < nt; ++t) {
+        list_start[t] = (int32_t)cnt[(size_t)t];
+        const int64_t c = cnt[(size_t)t + 1] - cnt[(size_t)t];
+        if (c > 0) busy.push_back({-c, (int32_t)t});
+        else empty.push_back((int32_t)t);
+    }
+    list_start[nt] = (int32_t)total;
+    std::stable_sort(busy.begin(), busy.end(),
+                     [](const std::pair<int64_t, int32_t>& x, const std::pair<int64_t, int32_t>& y) {
+                         return x.first < y.first;
+                     });
+    B.n_busy = (int64_t)busy.size();
+    for (size_t i = 0; i < busy.size(); ++i) order[i] = busy[i].second;
+    for (size_t i = 0; i < empty.size(); ++i) order[busy.size() + i] = empty[i];
+    // work items: lists longer than `split` entries become ranges of `split`;
+    // their partial tiles (64 points x ncol) live in the y-pass buffer, which
+    // holds n[0] * os[1] * os[2] points per column, so the split is widened
+    // until the partials fit
+    const int64_t max_slots = (int64_t)p->n[0] * p->os[1] * p->os[2] / 64;
+    int64_t split = kSplitEntries;
+    auto extra_slots = [&](int64_t sp) {
+        int64_t e = 0;
+        for (const auto& w : busy) e += (-w.first + sp - 1) / sp - 1;
+        return e;
+    };
+    while (extra_slots(split) > max_slots) split *= 2;
+    B.work_offset = (int64_t)work.size();
+    B.split_offset = (int64_t)splits.size();
+    int32_t slot = 0;
+    for (const auto& w : busy) {
+        const int64_t c = -w.first;
+        const int32_t t = w.second;
+        const int32_t beg = list_start[t];
+        const int64_t ns = (c + split - 1) / split;
+        if (ns > 1) splits.push_back(make_int4(t, slot, (int)(ns - 1), 0));
+        for (int64_t r = 0; r < ns; ++r) {
+            const int32_t b0 = beg + (int32_t)(r * split);
+            const int32_t b1 = beg + (int32_t)std::min<int64_t>(c, (r + 1) * split);
+            work.push_back(make_int4(t, b0, b1, r == 0 ? -1 : slot++));
+        }
+    }
+    B.n_work = (int64_t)work.size() - B.work_offset;
+    B.n_split = (int64_t)splits.size() - B.split_offset;
+    return TR_OK;
+}
 
 static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
     if (!d || !out) return fail(TR_ERR_INVALID_ARG, "tr_plan_create: null argument");
@@ -1507,8 +1726,11 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
     // scale coordinates exactly as the reference (float32 multiply, then add)
     std::vector<float4> ks_sorted((size_t)std::max<int64_t>(off, 1));
     std::vector<int32_t> perm((size_t)std::max<int64_t>(off, 1));
-    std::vector<int32_t> tstart((size_t)(p->ntiles + 1) * d->n_bins);
+    std::vector<int32_t> tstart((size_t)(p->ntiles + 1));
+    std::vector<int32_t> lstart((size_t)(p->ntiles + 1) * d->n_bins);
     std::vector<int32_t> torder((size_t)p->ntiles * d->n_bins);
+    std::vector<int2> glist;
+    std::vector<int4> gwork, gsplits;
     float scale[3], shift[3];
     for (int i = 0; i < 3; ++i) {
         scale[i] = (float)((double)p->os[i] / (double)p->n[i]);
@@ -1539,7 +1761,7 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
             key[(size_t)m] = (tcoord[0] * p->ntile[1] + tcoord[1]) * p->ntile[2] + tcoord[2];
         }
         // stable counting sort by tile
-        int32_t* ts = &tstart[(size_t)b * (p->ntiles + 1)];
+        int32_t* ts = tstart.data();
         std::fill(ts, ts + p->ntiles + 1, 0);
         for (int64_t m = 0; m < M; ++m) ts[key[(size_t)m] + 1]++;
         for (int64_t t = 0; t < p->ntiles; ++t) ts[t + 1] += ts[t];
@@ -1549,35 +1771,23 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
             perm[(size_t)(o + pos)] = (int32_t)m;
             ks_sorted[(size_t)(o + pos)] = kscaled[(size_t)m];
         }
-        // work queue: tiles ordered by candidate count (27 neighbours), heaviest first
-        std::vector<std::pair<int64_t, int32_t>> work((size_t)p->ntiles);
-        for (int tz = 0; tz < p->ntile[0]; ++tz)
-            for (int ty = 0; ty < p->ntile[1]; ++ty)
-                for (int tx = 0; tx < p->ntile[2]; ++tx) {
-                    int64_t cnt = 0;
-                    for (int dz = -1; dz <= 1; ++dz)
-                        for (int dy = -1; dy <= 1; ++dy)
-                            for (int dx = -1; dx <= 1; ++dx) {
-                                int nz = (tz + dz + p->ntile[0]) % p->ntile[0];
-                                int ny = (ty + dy + p->ntile[1]) % p->ntile[1];
-                                int nx = (tx + dx + p->ntile[2]) % p->ntile[2];
-                                int id = (nz * p->ntile[1] + ny) * p->ntile[2] + nx;
-                                cnt += ts[id + 1] - ts[id];
-                            }
-                    const int32_t id = (tz * p->ntile[1] + ty) * p->ntile[2] + tx;
-                    work[(size_t)id] = {-cnt, id};
-                }
-        std::stable_sort(work.begin(), work.end(),
-                         [](const std::pair<int64_t, int32_t>& x, const std::pair<int64_t, int32_t>& y) {
-                             return x.first < y.first;
-                         });
-        for (int64_t t = 0; t < p->ntiles; ++t) torder[(size_t)b * p->ntiles + t] = work[(size_t)t].second;
+        // gather lists: every (tile, sample) pair where the sample's KB support meets the tile
+        const tr_status lrc = build_gather_lists(p, b, M ? &ks_sorted[(size_t)o] : nullptr, M, glist,
+                                                 &lstart[(size_t)b * (p->ntiles + 1)], &torder[(size_t)b * p->ntiles],
+                                                 gwork, gsplits);
+        if (lrc != TR_OK) {
+            plan_free(p);
+            return lrc;
+        }
     }
     const size_t nks = (size_t)std::max<int64_t>(off, 1);
     if (cudaMalloc(&p->ks, nks * sizeof(float4)) != cudaSuccess ||
         cudaMalloc(&p->taps, nks * sizeof(TapRec)) != cudaSuccess ||
         cudaMalloc(&p->perm, nks * sizeof(int32_t)) != cudaSuccess ||
-        cudaMalloc(&p->tile_start, tstart.size() * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&p->glist, std::max<size_t>(glist.size(), 1) * sizeof(int2)) != cudaSuccess ||
+        cudaMalloc(&p->list_start, lstart.size() * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&p->work, std::max<size_t>(gwork.size(), 1) * sizeof(int4)) != cudaSuccess ||
+        cudaMalloc(&p->splits, std::max<size_t>(gsplits.size(), 1) * sizeof(int4)) != cudaSuccess ||
         cudaMalloc(&p->tile_order, torder.size() * sizeof(int32_t)) != cudaSuccess)
         return bad(TR_ERR_OOM, "allocation of the sorted trajectory failed");
     TR_CUDA(cudaMemcpy(p->ks, ks_sorted.data(), nks * sizeof(float4), cudaMemcpyHostToDevice));
@@ -1585,13 +1795,24 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
     k_prep_taps<<<(unsigned)((nks + 255) / 256), 256>>>(p->ks, (int64_t)nks, p->beta, (TapRec*)p->taps);
     TR_CHECK_LAUNCH();
     TR_CUDA(cudaDeviceSynchronize());
-    TR_CUDA(cudaMemcpy(p->tile_start, tstart.data(), tstart.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    if (!glist.empty())
+        TR_CUDA(cudaMemcpy(p->glist, glist.data(), glist.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    TR_CUDA(cudaMemcpy(p->list_start, lstart.data(), lstart.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    if (!gwork.empty())
+        TR_CUDA(cudaMemcpy(p->work, gwork.data(), gwork.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    if (!gsplits.empty())
+        TR_CUDA(cudaMemcpy(p->splits, gsplits.data(), gsplits.size() * sizeof(int4), cudaMemcpyHostToDevice));
     TR_CUDA(cudaMemcpy(p->tile_order, torder.data(), torder.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     if (cudaMalloc(&p->tol_dev, 4 * sizeof(double)) != cudaSuccess ||
-        cudaMallocHost(&p->tol_host, 4 * sizeof(double)) != cudaSuccess)
+        cudaMallocHost(&p->tol_host, 4 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&p->dev_err, sizeof(int)) != cudaSuccess || cudaMallocHost(&p->err_host, sizeof(int)) != cudaSuccess)
         return bad(TR_ERR_OOM, "allocation of reduction scalars failed");
+    TR_CUDA(cudaMemset(p->dev_err, 0, sizeof(int)));
+    *p->err_host = 0;
+    p->use_tma = (d->flags & TR_PLAN_NO_TMA) == 0;
     p->workspace_bytes = (int64_t)(nks * (sizeof(float4) + sizeof(TapRec) + sizeof(int32_t)) +
-                                   (tstart.size() + torder.size()) * sizeof(int32_t));
+                                   glist.size() * sizeof(int2) + (gwork.size() + gsplits.size()) * sizeof(int4) +
+                                   (lstart.size() + torder.size()) * sizeof(int32_t));
     TR_TRY(wavelet_prepare(p));
     *out = p;
     return TR_OK;

@@ -368,6 +368,7 @@ static tr_status enqueue_iteration(tr_plan* p, const tr_pdhg_state* s, const tr_
     k_tol_finalize<<<1, 256, 0, st>>>(p->partials, (int)blocks, p->tol_dev);
     TR_CHECK_LAUNCH();
     TR_CUDA(cudaMemcpyAsync(p->tol_host, p->tol_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    TR_CUDA(cudaMemcpyAsync(p->err_host, p->dev_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     return TR_OK;
 }
 
@@ -420,6 +421,14 @@ static tr_status run_impl(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_para
             TR_TRY(enqueue_iteration(p, s, q, st));
         }
         TR_CUDA(cudaStreamSynchronize(st));
+        if (*p->err_host != 0) {
+            const int bits = *p->err_host;
+            *p->err_host = 0;
+            cudaMemsetAsync(p->dev_err, 0, sizeof(int), st);
+            if (done) *done = it;
+            return fail(TR_ERR_TIMEOUT, "a bounded device wait expired in iteration " + std::to_string(it) +
+                                            " (error bits " + std::to_string(bits) + "); results are invalid");
+        }
         const double t = tolerance_from(q, p->tol_host[0], p->tol_host[1]);
         if (hist) hist[it] = t;
         if (!std::isfinite(p->tol_host[0]) || !std::isfinite(p->tol_host[1])) {

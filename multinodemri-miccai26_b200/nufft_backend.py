@@ -162,7 +162,7 @@ class B200NufftBackend(NufftBackend):
     """
 
     def __init__(self, img_shape, coordinates, device=0, *, dcf: Iterable | None = None, n_coils: int = 1,
-                 n_echoes: int = 1, autotune: bool = False) -> None:
+                 n_echoes: int = 1, autotune: bool = False, tma: bool = True) -> None:
         super().__init__(img_shape)
         import torch
         self._torch = torch
@@ -203,7 +203,7 @@ class B200NufftBackend(NufftBackend):
         desc.oversamp = 1.25
         desc.width = 4
         desc.device = self.device_index
-        desc.flags = _lib.TR_PLAN_AUTOTUNE if autotune else 0
+        desc.flags = (_lib.TR_PLAN_AUTOTUNE if autotune else 0) | (0 if tma else _lib.TR_PLAN_NO_TMA)
         handle = ctypes.c_void_p()
         _lib.check(lib.tr_plan_create(ctypes.byref(desc), ctypes.byref(handle)), "tr_plan_create")
         self._plan = handle
