@@ -110,6 +110,7 @@ struct FwdXArgs {
     FftStages S;
     float2* out;            // (Z, Y, OSX, ncol)
     int ncol;
+    int* err;               // device error word (kDevErr* bits)
 };
 
 __global__ void __launch_bounds__(256) k_fwd_x(FwdXArgs a) {
@@ -257,6 +258,7 @@ struct AdjXArgs {
     float2* img;            // (n_img, Z, Y, X)
     int64_t img_stride;
     int accumulate;
+    int* err;               // device error word (kDevErr* bits)
 };
 
 __global__ void __launch_bounds__(256) k_adj_x(AdjXArgs a) {
@@ -701,6 +703,141 @@ __global__ void __launch_bounds__(256) k_adj_x_st(AdjXArgs a) {
     }
 }
 
+// ------------------------------------------------------------------ TMA x-pass variants
+// One image row x W coils per CTA (W = CC).  Forward: the image row and the
+// row's W coil-map columns arrive by TMA in the FFT's second buffer, the
+// product (apodisation, scale, centred zero-pad) fills the first, and the
+// transformed [L][W] tile leaves as two TMA boxes of L/2 rows (the centred
+// shift g = (k + L/2) mod L splits it in two).  Adjoint: per coil group the
+// [L][W] tile arrives as two boxes (rows rotated by L/2), the inverse FFT
+// writes the cropped row into shared memory, and the conj(S) product and the
+// coil sum run as in k_adj_x_st.  Loads complete on one mbarrier (phase per
+// coil group) with a bounded wait.
+__device__ __forceinline__ float2* align128(unsigned char* p) {
+    return reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(p) + 127) & ~uintptr_t(127));
+}
+
+template <int L, int W>
+__global__ void __launch_bounds__(256) k_fwd_x_tma(FwdXArgs a, const __grid_constant__ CUtensorMap timg,
+                                                   const __grid_constant__ CUtensorMap tmap,
+                                                   const __grid_constant__ CUtensorMap tout) {
+    extern __shared__ __align__(128) unsigned char xsm_raw[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ float s_apzy;
+    float2* sm = align128(xsm_raw);
+    float2* smA = sm;
+    float2* smB = sm + L * W;
+    float2* tws = sm + 2 * L * W;
+    const int X = a.X;
+    float2* s_img = smB;              // [X]
+    float2* s_map = smB + X;          // [X][W]
+    const int img = (int)(blockIdx.x % (unsigned)a.n_img);
+    const int row = (int)(blockIdx.x / (unsigned)a.n_img);
+    const int c0 = (int)blockIdx.z * W;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(&bar, (unsigned)(X * (W + 1) * sizeof(float2)));
+        tma_load_3d(s_img, &timg, &bar, 0, row, img);
+        tma_load_3d(s_map, &tmap, &bar, c0, 0, row);
+        const int z = row / a.Y, y = row - z * a.Y;
+        s_apzy = a.apz[z] * a.apy[y] * a.scale;
+    }
+    for (int i = threadIdx.x; i < L; i += 256) tws[i] = a.tw[i];
+    const bool ok = mbar_wait_bounded(&bar, 0, kMbarPollLimit);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
+        return;
+    }
+    const float apzy = s_apzy;
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < L * W; idx += 256) {
+        const int m = idx / W, w = idx - m * W;
+        int j = m + a.h;
+        if (j >= L) j -= L;
+        const int x = j - a.pad;
+        float2 v = make_float2(0.f, 0.f);
+        if (x >= 0 && x < X) v = cscale(cmul(s_img[x], s_map[x * W + w]), apzy * a.apx[x]);
+        smA[idx] = v;
+    }
+    __syncthreads();
+    float2* ep = fft_ct_free<L>(smA, smB);
+    auto store = [ep](int k, int w, float2 v) { ep[k * W + w] = v; };
+    fft_ct<L, W, 256, false>(smA, smB, tws, store);
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int col = img * a.C + c0;
+        tma_store_3d(&tout, ep + (L / 2) * W, col, 0, row);
+        tma_store_3d(&tout, ep, col, L / 2, row);
+        tma_store_commit_and_drain();
+    }
+}
+
+template <int L, int W>
+__global__ void __launch_bounds__(256, 4) k_adj_x_tma(AdjXArgs a, const __grid_constant__ CUtensorMap tin) {
+    extern __shared__ __align__(128) unsigned char xsm_raw[];
+    __shared__ __align__(8) uint64_t bar;
+    float2* sm = align128(xsm_raw);
+    float2* buf0 = sm;
+    float2* buf1 = sm + L * W;
+    float2* tws = sm + 2 * L * W;
+    float2* acc = tws + L;                  // [X]
+    const int X = a.X;
+    const int img = (int)(blockIdx.x % (unsigned)a.n_img);
+    const int row = (int)(blockIdx.x / (unsigned)a.n_img);
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    for (int i = threadIdx.x; i < L; i += 256) tws[i] = a.tw[i];
+    for (int i = threadIdx.x; i < X; i += 256) acc[i] = make_float2(0.f, 0.f);
+    float2* ep = fft_ct_free<L>(buf0, buf1);
+    const int shift = a.h - a.pad;
+    int phase = 0;
+    for (int c0 = 0; c0 < a.C; c0 += W, phase ^= 1) {
+        __syncthreads();                    // the previous group's readers of buf0 / ep are done
+        if (threadIdx.x == 0) {
+            mbar_expect_tx(&bar, (unsigned)(L * W * sizeof(float2)));
+            const int col = img * a.C + c0;
+            tma_load_3d(buf0, &tin, &bar, col, L / 2, row);
+            tma_load_3d(buf0 + (L / 2) * W, &tin, &bar, col, 0, row);
+        }
+        const bool ok = mbar_wait_bounded(&bar, (unsigned)phase, kMbarPollLimit);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
+            return;
+        }
+        auto store = [&](int k, int w, float2 v) {
+            int o = k + shift;
+            o = o >= L ? o - L : (o < 0 ? o + L : o);
+            if (o < X) ep[o * W + w] = v;
+        };
+        fft_ct<L, W, 256, true>(buf0, buf1, tws, store);
+        __syncthreads();
+        // thread (x, w): conj(S) product, then a sum over the W lanes of the group
+        for (int base = 0; base < X * W; base += 256) {
+            const int i = base + (int)threadIdx.x;
+            const bool live = i < X * W;
+            const int x = i / W, w = i - x * W;
+            float2 v = make_float2(0.f, 0.f);
+            if (live) v = cmulc(ep[i], a.maps[((int64_t)row * X + x) * a.C + c0 + w]);
+#pragma unroll
+            for (int o = W / 2; o > 0; o >>= 1) {
+                v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+                v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+            }
+            if (live && w == 0) acc[x] = cadd(acc[x], v);
+        }
+    }
+    __syncthreads();
+    const int z = row / a.Y, y = row - z * a.Y;
+    const float szy = a.apz[z] * a.apy[y] * a.scale;
+    for (int x = threadIdx.x; x < X; x += 256) {
+        float2 v = cscale(acc[x], szy * a.apx[x]);
+        float2* dst = a.img + (int64_t)img * a.img_stride + (int64_t)row * X + x;
+        if (a.accumulate) v = cadd(*dst, v);
+        *dst = v;
+    }
+}
+
 // ------------------------------------------------------------------ per-sample tap records
 // First tap per axis and the 15 KB weights of every (sorted) sample, computed
 // once at plan creation; interpolation and gridding read them instead of
@@ -876,7 +1013,7 @@ __device__ __forceinline__ void tile_geometry(const SpreadArgs& a, int tile, int
 }
 
 template <int CG>
-__global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
+__global__ void __launch_bounds__(256, (CG >= 6 ? 3 : 4)) k_spread(SpreadArgs a) {
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ int l_rel[kSpreadSub];
     float* c_w = reinterpret_cast<float*>(smraw);                        // [kSpreadSub][16]
@@ -932,12 +1069,11 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
             reinterpret_cast<float4*>(c_w)[cand * 4 + part] = a.taps[e.x].w[part];
             if (part == 0) l_rel[cand] = e.y;
         }
-        for (int i = tid; i < ns * ncc; i += 256) {
-            const int cand = i / ncc, col = i - cand * ncc;
+        for (int cand = tid >> 5; cand < ns; cand += 8) {     // one warp per entry, lanes over columns
             const int sm = a.list[base + cand].x;
-            float2 v = a.vals[(int64_t)sm * a.ncol + col0 + col];
-            if (a.use_dcf) v = cscale(v, a.ks[sm].w);
-            dq[i] = v;
+            const float2* src = a.vals + (int64_t)sm * a.ncol + col0;
+            const float dw = a.use_dcf ? a.ks[sm].w : 1.0f;
+            for (int col = tid & 31; col < ncc; col += 32) dq[cand * ncc + col] = cscale(src[col], dw);
         }
         __syncthreads();
         for (int cc = 0; cc < ns; ++cc) {
@@ -966,23 +1102,34 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs a) {
         }
         __syncthreads();
     }
-    // ---- write the tile (or the partial tile of a split list): 4 x-points x CG columns
-    if (slot >= 0) {
-        float2* dst = a.partials + ((int64_t)slot * 64 + row * 4) * a.ncol + col0 + c_lo;
+    // ---- stage the tile as [64 points][ncc] in shared memory (the value buffer
+    // holds kSpreadSub * ncc >= 64 * ncc), then store it coalesced, one warp per
+    // point; a split list's partial tile goes to its slot instead of the grid
+    static_assert(kSpreadSub >= 64, "the value buffer must hold a whole tile");
+    __syncthreads();
 #pragma unroll
-        for (int x = 0; x < 4; ++x)
+    for (int x = 0; x < 4; ++x)
 #pragma unroll
-            for (int j = 0; j < CG; ++j)
-                if (c_lo + j < ncc) dst[(int64_t)x * a.ncol + j] = acc[x][j];
-    } else if (pz < Tz && py < Ty) {
-        const int64_t rowg = ((int64_t)(t0z + pz) * a.os1 + (t0y + py)) * a.os2 + t0x;
-#pragma unroll
-        for (int x = 0; x < 4; ++x) {
-            if (x >= Tx) continue;
-            float2* dst = a.grid + (rowg + x) * a.ncol + col0 + c_lo;
-#pragma unroll
-            for (int j = 0; j < CG; ++j)
-                if (c_lo + j < ncc) dst[j] = acc[x][j];
+        for (int j = 0; j < CG; ++j)
+            if (c_lo + j < ncc) dq[(row * 4 + x) * ncc + c_lo + j] = acc[x][j];
+    __syncthreads();
+    const int warp = tid >> 5, lane = tid & 31;
+    const bool vec = ((ncc | a.ncol | col0) & 1) == 0;
+    for (int pt = warp; pt < 64; pt += 8) {
+        const int qz = pt >> 4, qy = (pt >> 2) & 3, qx = pt & 3;
+        float2* dst;
+        if (slot >= 0) {
+            dst = a.partials + ((int64_t)slot * 64 + pt) * a.ncol + col0;
+        } else {
+            if (qz >= Tz || qy >= Ty || qx >= Tx) continue;
+            dst = a.grid + (((int64_t)(t0z + qz) * a.os1 + (t0y + qy)) * a.os2 + (t0x + qx)) * a.ncol + col0;
+        }
+        const float2* src = dq + pt * ncc;
+        if (vec) {
+            for (int c = lane; c < (ncc >> 1); c += 32)
+                reinterpret_cast<float4*>(dst)[c] = reinterpret_cast<const float4*>(src)[c];
+        } else {
+            for (int c = lane; c < ncc; c += 32) dst[c] = src[c];
         }
     }
 }
@@ -1221,6 +1368,39 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
     fa.S = stages_of(p->ax[2]);
     fa.out = p->bufA;
     fa.ncol = n_img * C;
+    fa.err = p->dev_err;
+    // TMA variant: one image row x Wct coils per CTA
+    if (p->use_tma && ct && maps && C % Wct == 0 && X % 16 == 0 && X <= 256 && img_stride % 2 == 0 &&
+        (int64_t)X * (Wct + 1) <= (int64_t)OSX * Wct && OSX / 2 <= 256) {
+        CUtensorMap timg, tmap, tout;
+        const uint64_t nrows = (uint64_t)Z * Y;
+        PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+        bool ok = enc != nullptr;
+        if (ok) {
+            const cuuint64_t dims[3] = {(cuuint64_t)X, nrows, (cuuint64_t)n_img};
+            const cuuint64_t strides[2] = {(cuuint64_t)X * 8, (cuuint64_t)img_stride * 8};
+            const cuuint32_t box[3] = {(cuuint32_t)X, 1, 1};
+            const cuuint32_t estr[3] = {1, 1, 1};
+            ok = enc(&timg, CU_TENSOR_MAP_DATA_TYPE_INT64, 3, const_cast<float2*>(images), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+        }
+        ok = ok && encode_map_3d(&tmap, maps, (uint64_t)C, (uint64_t)X, nrows, (uint32_t)Wct, (uint32_t)X);
+        ok = ok && encode_map_3d(&tout, p->bufA, (uint64_t)fa.ncol, (uint64_t)OSX, nrows, (uint32_t)Wct,
+                                 (uint32_t)(OSX / 2));
+        const void* tfn = nullptr;
+#define TR_FWDX_TMA(LV) case LV: tfn = (const void*)k_fwd_x_tma<LV, ct_width(LV)>; break;
+        switch (OSX) { TR_CT_LENGTHS(TR_FWDX_TMA) default: break; }
+#undef TR_FWDX_TMA
+        if (ok && tfn) {
+            const size_t smem = fft_smem_bytes(OSX, Wct) + 128;
+            TR_TRY(set_smem_limit(tfn, smem));
+            dim3 grid((unsigned)(nrows * n_img), 1u, (unsigned)(C / Wct));
+            void* args[] = {&fa, &timg, &tmap, &tout};
+            TR_CUDA(cudaLaunchKernel(tfn, grid, dim3(256), args, smem, st));
+            return TR_OK;
+        }
+    }
     const int W = fa.rows * fa.cc;
     const size_t smem = fft_smem_bytes(OSX, W);
     // the n_img CTAs of one row block are adjacent, so the coil-map rows they share come from L2
@@ -1380,6 +1560,24 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
     aa.img = images;
     aa.img_stride = img_stride;
     aa.accumulate = 0;
+    aa.err = p->dev_err;
+    // TMA variant: one image row per CTA, coil groups of Wct
+    if (p->use_tma && ct && maps && C % Wct == 0 && OSX / 2 <= 256) {
+        CUtensorMap tin;
+        const void* tfn = nullptr;
+#define TR_ADJX_TMA(LV) case LV: tfn = (const void*)k_adj_x_tma<LV, ct_width(LV)>; break;
+        switch (OSX) { TR_CT_LENGTHS(TR_ADJX_TMA) default: break; }
+#undef TR_ADJX_TMA
+        if (tfn && encode_map_3d(&tin, p->bufA, (uint64_t)aa.ncol, (uint64_t)OSX, (uint64_t)Z * Y, (uint32_t)Wct,
+                                 (uint32_t)(OSX / 2))) {
+            const size_t smem = fft_smem_bytes(OSX, Wct) + (size_t)X * sizeof(float2) + 128;
+            TR_TRY(set_smem_limit(tfn, smem));
+            dim3 grid((unsigned)((int64_t)Z * Y * n_img));
+            void* args[] = {&aa, &tin};
+            TR_CUDA(cudaLaunchKernel(tfn, grid, dim3(256), args, smem, st));
+            return TR_OK;
+        }
+    }
     const int W = aa.rows * aa.cc;
     const size_t smem = fft_smem_bytes(OSX, W) + (size_t)aa.rows * X * sizeof(float2);
     dim3 grid((unsigned)(((Z * Y + aa.rows - 1) / aa.rows) * n_img));
