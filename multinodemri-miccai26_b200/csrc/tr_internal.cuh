@@ -42,6 +42,22 @@ __host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return mak
 __host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+// c + w * v on both components with one packed f32x2 FMA (sm_100); the same
+// single rounding per component as two scalar FMAs.
+__device__ __forceinline__ float2 cfma_real(float w, float2 v, float2 c) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    unsigned long long rw, rv, rc, rd;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(rw) : "f"(w));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(rv) : "f"(v.x), "f"(v.y));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(rc) : "f"(c.x), "f"(c.y));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(rd) : "l"(rw), "l"(rv), "l"(rc));
+    float2 d;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(rd));
+    return d;
+#else
+    return make_float2(fmaf(w, v.x, c.x), fmaf(w, v.y, c.y));
+#endif
+}
 // a * conj(b)
 __host__ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
     return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);

@@ -775,22 +775,24 @@ __global__ void __launch_bounds__(256) k_fwd_x_tma(FwdXArgs a, const __grid_cons
 }
 
 template <int L, int W>
-__global__ void __launch_bounds__(256, 4) k_adj_x_tma(AdjXArgs a, const __grid_constant__ CUtensorMap tin) {
+__global__ void __launch_bounds__(256, (W >= 16 ? 3 : 4)) k_adj_x_tma(AdjXArgs a, const __grid_constant__ CUtensorMap tin) {
     extern __shared__ __align__(128) unsigned char xsm_raw[];
     __shared__ __align__(8) uint64_t bar;
     float2* sm = align128(xsm_raw);
     float2* buf0 = sm;
     float2* buf1 = sm + L * W;
     float2* tws = sm + 2 * L * W;
-    float2* acc = tws + L;                  // [X]
-    const int X = a.X;
+    const int X = a.X;                      // <= 256: thread x owns image column x
+    const int XP = X + 4;                   // padded row of the [W][XP] epilogue tile
     const int img = (int)(blockIdx.x % (unsigned)a.n_img);
     const int row = (int)(blockIdx.x / (unsigned)a.n_img);
+    const int x = threadIdx.x;
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     for (int i = threadIdx.x; i < L; i += 256) tws[i] = a.tw[i];
-    for (int i = threadIdx.x; i < X; i += 256) acc[i] = make_float2(0.f, 0.f);
     float2* ep = fft_ct_free<L>(buf0, buf1);
     const int shift = a.h - a.pad;
+    const float4* mrow = reinterpret_cast<const float4*>(a.maps + ((int64_t)row * X + x) * a.C);
+    float2 s = make_float2(0.f, 0.f);
     int phase = 0;
     for (int c0 = 0; c0 < a.C; c0 += W, phase ^= 1) {
         __syncthreads();                    // the previous group's readers of buf0 / ep are done
@@ -800,6 +802,12 @@ __global__ void __launch_bounds__(256, 4) k_adj_x_tma(AdjXArgs a, const __grid_c
             tma_load_3d(buf0, &tin, &bar, col, L / 2, row);
             tma_load_3d(buf0 + (L / 2) * W, &tin, &bar, col, 0, row);
         }
+        // this column's W coil-map values, in flight during the transform
+        float4 m2[W / 2];
+        if (x < X) {
+#pragma unroll
+            for (int q = 0; q < W / 2; ++q) m2[q] = mrow[(c0 >> 1) + q];
+        }
         const bool ok = mbar_wait_bounded(&bar, (unsigned)phase, kMbarPollLimit);
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
@@ -808,30 +816,22 @@ __global__ void __launch_bounds__(256, 4) k_adj_x_tma(AdjXArgs a, const __grid_c
         auto store = [&](int k, int w, float2 v) {
             int o = k + shift;
             o = o >= L ? o - L : (o < 0 ? o + L : o);
-            if (o < X) ep[o * W + w] = v;
+            if (o < X) ep[w * XP + o] = v;
         };
         fft_ct<L, W, 256, true>(buf0, buf1, tws, store);
         __syncthreads();
-        // thread (x, w): conj(S) product, then a sum over the W lanes of the group
-        for (int base = 0; base < X * W; base += 256) {
-            const int i = base + (int)threadIdx.x;
-            const bool live = i < X * W;
-            const int x = i / W, w = i - x * W;
-            float2 v = make_float2(0.f, 0.f);
-            if (live) v = cmulc(ep[i], a.maps[((int64_t)row * X + x) * a.C + c0 + w]);
+        // conj(S) product and the sum over this group's coils, in coil order
+        if (x < X) {
 #pragma unroll
-            for (int o = W / 2; o > 0; o >>= 1) {
-                v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
-                v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+            for (int q = 0; q < W / 2; ++q) {
+                s = cadd(s, cmulc(ep[(2 * q) * XP + x], make_float2(m2[q].x, m2[q].y)));
+                s = cadd(s, cmulc(ep[(2 * q + 1) * XP + x], make_float2(m2[q].z, m2[q].w)));
             }
-            if (live && w == 0) acc[x] = cadd(acc[x], v);
         }
     }
-    __syncthreads();
-    const int z = row / a.Y, y = row - z * a.Y;
-    const float szy = a.apz[z] * a.apy[y] * a.scale;
-    for (int x = threadIdx.x; x < X; x += 256) {
-        float2 v = cscale(acc[x], szy * a.apx[x]);
+    if (x < X) {
+        const int z = row / a.Y, y = row - z * a.Y;
+        float2 v = cscale(s, a.apz[z] * a.apy[y] * a.scale * a.apx[x]);
         float2* dst = a.img + (int64_t)img * a.img_stride + (int64_t)row * X + x;
         if (a.accumulate) v = cadd(*dst, v);
         *dst = v;
@@ -907,9 +907,7 @@ __global__ void __launch_bounds__(256) k_interp(const float2* __restrict__ grid,
                     for (int j = 0; j < CPL; ++j) {
                         const int col = lane + j * G;
                         if (col < ncol) {
-                            const float2 g = gp[col];
-                            acc[j].x += w * g.x;
-                            acc[j].y += w * g.y;
+                            acc[j] = cfma_real(w, gp[col], acc[j]);
                         }
                     }
                 }
@@ -934,9 +932,7 @@ __global__ void __launch_bounds__(256) k_interp(const float2* __restrict__ grid,
                 for (int j = 0; j < CPL; ++j) {
                     const int col = lane + j * G;
                     if (col < ncol) {
-                        const float2 g = gp[col];
-                        acc[j].x += w * g.x;
-                        acc[j].y += w * g.y;
+                        acc[j] = cfma_real(w, gp[col], acc[j]);
                     }
                 }
             }
@@ -1016,6 +1012,8 @@ template <int CG>
 __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : 4)) k_spread(SpreadArgs a) {
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ int l_rel[kSpreadSub];
+    __shared__ float s_wzy[kSpreadSub * 16];
+    __shared__ __align__(16) float s_wx[kSpreadSub * 4];
     float* c_w = reinterpret_cast<float*>(smraw);                        // [kSpreadSub][16]
     float2* dq = reinterpret_cast<float2*>(c_w + 16 * kSpreadSub);       // [kSpreadSub][ncc]
     const int tid = threadIdx.x;
@@ -1051,8 +1049,7 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : 4)) k_spread(SpreadArgs a)
     int t0z, t0y, t0x, Tz, Ty, Tx;
     tile_geometry(a, tile, t0z, t0y, t0x, Tz, Ty, Tx);
 
-    const int row = tid >> 4;
-    const int pz = row >> 2, py = row & 3;
+    const int row = tid >> 4;          // tile row (z, y) = (row / 4, row % 4)
     const int g = tid & 15;
     const int c_lo = g * CG;
     float2 acc[4][CG];
@@ -1076,28 +1073,36 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : 4)) k_spread(SpreadArgs a)
             for (int col = tid & 31; col < ncc; col += 32) dq[cand * ncc + col] = cscale(src[col], dw);
         }
         __syncthreads();
+        // per entry: the (z, y) weight of each of the 16 tile rows and the x weight
+        // of each of the 4 tile columns (zero where the support misses the tile)
+        for (int i = tid; i < ns * 20; i += 256) {
+            const int cand = i / 20, k = i - cand * 20;
+            const int pk = l_rel[cand];
+            const float* w = c_w + 16 * cand;
+            if (k < 16) {
+                const int az = (pk & 0xff) - 128 + (k >> 2);
+                const int ay = ((pk >> 8) & 0xff) - 128 + (k & 3);
+                s_wzy[cand * 16 + k] = ((unsigned)az <= 4u && (unsigned)ay <= 4u) ? w[az] * w[5 + ay] : 0.f;
+            } else {
+                const int ax = ((pk >> 16) & 0xff) - 128 + (k - 16);
+                s_wx[cand * 4 + (k - 16)] = (unsigned)ax <= 4u ? w[10 + ax] : 0.f;
+            }
+        }
+        __syncthreads();
         for (int cc = 0; cc < ns; ++cc) {
-            const int pk = l_rel[cc];
-            const int az = (pk & 0xff) - 128 + pz;
-            const int ay = ((pk >> 8) & 0xff) - 128 + py;
-            if ((unsigned)az > 4u || (unsigned)ay > 4u) continue;
-            const float* w = c_w + 16 * cc;
-            const float wzy = w[az] * w[5 + ay];
+            const float wzy = s_wzy[cc * 16 + row];
             if (wzy == 0.f) continue;
-            const int rx = ((pk >> 16) & 0xff) - 128;
+            const float4 wx4 = reinterpret_cast<const float4*>(s_wx)[cc];
+            const float wx[4] = {wx4.x, wx4.y, wx4.z, wx4.w};
             float2 v[CG];
 #pragma unroll
             for (int j = 0; j < CG; ++j) v[j] = (c_lo + j < ncc) ? dq[cc * ncc + c_lo + j] : make_float2(0.f, 0.f);
 #pragma unroll
             for (int x = 0; x < 4; ++x) {
-                const int ax = rx + x;
-                if ((unsigned)ax > 4u) continue;
-                const float wt = wzy * w[10 + ax];
+                if (wx[x] == 0.f) continue;
+                const float wt = wzy * wx[x];
 #pragma unroll
-                for (int j = 0; j < CG; ++j) {
-                    acc[x][j].x += wt * v[j].x;
-                    acc[x][j].y += wt * v[j].y;
-                }
+                for (int j = 0; j < CG; ++j) acc[x][j] = cfma_real(wt, v[j], acc[x][j]);
             }
         }
         __syncthreads();
@@ -1562,7 +1567,7 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
     aa.accumulate = 0;
     aa.err = p->dev_err;
     // TMA variant: one image row per CTA, coil groups of Wct
-    if (p->use_tma && ct && maps && C % Wct == 0 && OSX / 2 <= 256) {
+    if (p->use_tma && ct && maps && C % Wct == 0 && OSX / 2 <= 256 && X <= 256 && X + 4 <= OSX) {
         CUtensorMap tin;
         const void* tfn = nullptr;
 #define TR_ADJX_TMA(LV) case LV: tfn = (const void*)k_adj_x_tma<LV, ct_width(LV)>; break;
@@ -1570,7 +1575,7 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
 #undef TR_ADJX_TMA
         if (tfn && encode_map_3d(&tin, p->bufA, (uint64_t)aa.ncol, (uint64_t)OSX, (uint64_t)Z * Y, (uint32_t)Wct,
                                  (uint32_t)(OSX / 2))) {
-            const size_t smem = fft_smem_bytes(OSX, Wct) + (size_t)X * sizeof(float2) + 128;
+            const size_t smem = fft_smem_bytes(OSX, Wct) + 128;
             TR_TRY(set_smem_limit(tfn, smem));
             dim3 grid((unsigned)((int64_t)Z * Y * n_img));
             void* args[] = {&aa, &tin};
