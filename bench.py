@@ -23,8 +23,10 @@ on the full workload) against the measured HBM copy bandwidth.
 a bounded sample (one bin-echo-coil forward + adjoint NUFFT at full size plus
 one PDHG elementwise slice) scaled to the solve.
 
-Multi-GPU (torchrun): replicas only -- each rank solves its own copy of the
-problem (the single-device path does not shard); times are the max over ranks.
+Multi-GPU (torchrun): the motion bins of the same problem are split over the
+ranks by sample count, with the one-bin halos of u_bar and p_m and the two
+stopping sums passed over NCCL each iteration (``parallel.py``); strong
+scaling, times are the max over ranks.
 Inputs exceed L2 (126 MB): every k-space column block and grid is larger.
 """
 
@@ -71,6 +73,8 @@ def parse(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--sharded", action="store_true",
+                    help="use the bin-sharded multi-GPU path even on one GPU (exercises its code on one device)")
     return ap.parse_args(argv)
 
 
@@ -148,14 +152,16 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(load), "sm_max_mhz": smax, "reasons": reasons, "samples": len(rows)}
 
 
-def dist_setup():
+def dist_setup(force: bool = False):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
+    if world > 1 or force:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if force and "MASTER_ADDR" not in os.environ:
+            os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": "29517", "RANK": "0", "WORLD_SIZE": "1"})
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -213,8 +219,13 @@ def bin_coords(ds):
 # --------------------------------------------------------------------------- b200 arm
 def run_b200(args):
     import torch
-    world, rank, local = dist_setup()
+    world, rank, local = dist_setup(force=args.sharded)
     torch.cuda.set_device(local)
+    if world > 1 or args.sharded:
+        run_b200_sharded(args, world, rank, local)
+        import torch.distributed as dist
+        dist.destroy_process_group()
+        return
     device = torch.device("cuda", local)
     syn = importlib.import_module(f"{PKG}.synthetic")
     solver_mod = importlib.import_module(f"{PKG}.solver")
@@ -336,7 +347,7 @@ def run_b200(args):
             "warmup": max(3, args.warmup),
             "ms_per_step": round(ms_step, 3),
             "higher_is_better": False,
-            "scaling": "weak",
+            "scaling": "strong",
             "vs_baseline": None,
             "dtype": "c64",
             "data": "synthetic",
@@ -368,6 +379,97 @@ def run_b200(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------------- b200 arm, several GPUs
+def run_b200_sharded(args, world, rank, local):
+    """N ranks, one GPU each: the motion bins of the one problem split by
+    sample count (``parallel.partition_bins``), halos and the stopping sums over
+    NCCL.  Strong scaling: the whole job is the same single problem."""
+    import torch
+    device = torch.device("cuda", local)
+    syn = importlib.import_module(f"{PKG}.synthetic")
+    solver_mod = importlib.import_module(f"{PKG}.solver")
+    par = importlib.import_module(f"{PKG}.parallel")
+    cfg = get_config(args)
+    ds = syn.make_geometry(cfg)
+    syn.simulate_kspace_b200(ds, local)
+    coords, dcfs, ksps = bin_coords(ds), ds.bin_dcf(), ds.bin_ksp()
+    counts = [int(np.prod(c.shape[:-1])) for c in coords]
+    ranges = par.partition_bins(counts, world)
+    a, e = ranges[rank]
+    lam = cfg.lam
+    comm = par.TorchHaloComm(ranges)
+
+    def build(mps, ksp_list):
+        if e <= a:
+            return None, par.IdleEngine(device)
+        sv = solver_mod.PdhgSolver(cfg.algorithm, cfg.img_shape, coords[a:e], dcfs[a:e], mps, ksp_list[a:e],
+                                   l2_coupling=cfg.l2_coupling, lam_m=lam, lam_e=lam, lam_w1=lam, lam_w2=lam,
+                                   device=local)
+        return sv, par.B200ShardEngine(sv, a, len(counts))
+
+    solver, eng = build(ds.mps, ksps)
+    sh = par.ShardedPdhg(eng, comm, cfg.algorithm)
+    clocks = ClockSampler(local)
+    eng.reset(None)
+    sh.iterate(max(3, args.warmup), 0.0, 1 / 6, 1 / 6)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    t = eng.timer()
+    t.start()
+    sh.iterate(args.steps, 0.0, 1 / 6, 1 / 6)
+    ms_step = max_over_ranks(t.stop() * 1e3 / args.steps, world, device)
+    res = sh.run(max_iter=cfg.max_iter, tol=cfg.tol)
+    t_plain = max_over_ranks(res.seconds, world, device)
+    clk = clocks.stop()
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda x: torch.from_numpy(np.ascontiguousarray(x)).pin_memory()
+        ksp_h = [pin(k) if a <= i < e else None for i, k in enumerate(ksps)]
+        mps_h = pin(ds.mps)
+        h2d = sum(k.numel() * 8 for k in ksp_h if k is not None) + mps_h.numel() * 8 + \
+            sum(c.size * 4 for c in coords[a:e]) + sum(d.size * 4 for d in dcfs[a:e])
+        if solver is not None:
+            solver.close()
+        del solver, eng, sh
+        torch.cuda.empty_cache()
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s2, eng2 = build(mps_h, ksp_h)
+        r2 = par.ShardedPdhg(eng2, comm, cfg.algorithm).run(max_iter=cfg.max_iter, tol=cfg.tol)
+        d2h = 0
+        if r2.image is not None:
+            out_h = torch.empty(r2.image.shape, dtype=torch.complex64, pin_memory=True)
+            out_h.copy_(r2.image, non_blocking=True)
+            d2h = out_h.numel() * 8
+        torch.cuda.synchronize()
+        t_e2e = max_over_ranks(time.perf_counter() - t0, world, device)
+        e2e = {"value": round(t_e2e, 4), "unit": "s", "h2d_bytes_per_step": int(max_over_ranks(h2d, world, device)),
+               "d2h_bytes_per_step": int(max_over_ranks(d2h, world, device))}
+        if s2 is not None:
+            s2.close()
+    if rank == 0:
+        E, C = cfg.n_echoes, cfg.n_coils
+        line = {
+            "metric": METRIC, "value": round(t_plain, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": round(ms_step, 3), "higher_is_better": False,
+            "scaling": "strong", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {"workload": cfg.name, "algorithm": cfg.algorithm, "img_shape_zyx": list(cfg.img_shape),
+                       "coils": C, "echoes": E, "bins": cfg.n_bins, "cones": cfg.n_interleaves,
+                       "readout": cfg.n_readout, "tol": cfg.tol, "max_iter": cfg.max_iter,
+                       "l2_flush": "inputs larger than L2",
+                       "parallelism": f"motion bins over {world} GPUs, NCCL halos",
+                       "bins_per_rank": [int(y - x) for x, y in ranges]},
+            "value_source": "plain PDHG",
+            "time_to_tol_plain_s": round(t_plain, 4), "iterations_plain": res.iterations,
+            "iterations_per_s": round(1000.0 / ms_step, 3),
+            "clocks": clk, "e2e": e2e, "cpu_baseline": None,
+            "gpu_launches": (max(e - a for a, e in ranges) * (8 + 1) + 3) * args.steps,
+        }
+        print(json.dumps(line), flush=True)
 
 
 # --------------------------------------------------------------------------- reference arm

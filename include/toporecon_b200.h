@@ -78,6 +78,7 @@ typedef struct {
     int32_t wavelet_levels;      /* db6 levels for TVMW (PyWavelets max level) */
     int64_t wavelet_coeffs;      /* db6 coefficients per (bin, echo) image */
     int32_t fft_line_width;      /* columns per CTA chosen for the FFT passes */
+    int32_t spread_columns;      /* k-space columns per gridding CTA (last tuned / used value) */
 } tr_plan_info_t;
 
 tr_status tr_plan_create(const tr_plan_desc* desc, tr_plan** out);
@@ -155,6 +156,34 @@ tr_status tr_plan_bin_offset(const tr_plan* plan, int32_t bin, int64_t* offset, 
 tr_status tr_pdhg_run(tr_plan* plan, const tr_pdhg_state* state, const tr_pdhg_params* params,
                       int32_t max_iters, double tol, double* tol_history, int32_t* iters_done,
                       void* stream);
+
+/* Bin-sharded PDHG: the motion bins of one problem spread over ranks, each
+ * rank with a plan holding a contiguous range of bins.  Replaces the
+ * reference's motion-axis halo exchange (u_bar forward ghost around the motion
+ * dual, tvme.py:217-229, tvm.py:230-260; p_m backward ghost around the motion
+ * divergence, tvme.py:421-437, tvm.py:342-357, tvmw.py:662-670) and the
+ * all-reduce of the stopping sums (tvme.py:518-551, tvm.py:406-472,
+ * tvmw.py:716-769). */
+typedef struct {
+    int32_t n_bins_global;       /* bins of the whole problem (>= bin_offset + the plan's bins) */
+    int32_t bin_offset;          /* global index of the plan's first bin */
+    const void* u_bar_next;      /* device (E, Z, Y, X) complex64: u_bar of the global bin after the plan's
+                                    last one; NULL when the plan holds the global last bin */
+    const void* p_m_prev;        /* device (E, Z, Y, X) complex64: p_m of the global bin before the plan's
+                                    first one; NULL when the plan holds bin 0 */
+} tr_pdhg_shard;
+
+/* One half of a PDHG iteration on the plan's bins, asynchronous on `stream`.
+ * phase 1: every dual update (data, motion / echo TV, wavelets) and the data
+ *          gradient; reads shard->u_bar_next.
+ * phase 2: primal update, extrapolation and the FP64 tolerance sums
+ *          (numerator, denominator) of the plan's bins into tol_sums[2]
+ *          (device memory) for the caller's all-reduce; reads shard->p_m_prev.
+ * Between the phases the caller passes its last p_m bin to the next rank; after
+ * phase 2 its first u_bar bin to the previous rank.  TR_ERR_TIMEOUT reports a
+ * device wait that expired in an earlier phase on this plan. */
+tr_status tr_pdhg_phase(tr_plan* plan, const tr_pdhg_state* state, const tr_pdhg_params* params,
+                        const tr_pdhg_shard* shard, int32_t phase, double* tol_sums, void* stream);
 
 /* Diagnostics in FP64: operator-norm estimate sqrt(||A^H W A||) of the data
  * term (A = [F_b S_c], W = density weights) by n_iter power-iteration steps

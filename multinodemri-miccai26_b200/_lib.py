@@ -30,7 +30,7 @@ EXPORTED = (
     "tr_plan_sort_kspace", "tr_plan_unsort_kspace", "tr_nufft_forward", "tr_nufft_adjoint",
     "tr_nufft_forward_bin", "tr_nufft_adjoint_bin", "tr_plan_bin_offset", "tr_pdhg_run",
     "tr_power_iteration", "tr_profile_nufft", "tr_tolerance_sums_noalloc", "tr_conv3d_fwd",
-    "tr_conv3d_wgrad_workspace", "tr_conv3d_wgrad",
+    "tr_conv3d_wgrad_workspace", "tr_conv3d_wgrad", "tr_pdhg_phase",
 )
 
 
@@ -70,6 +70,7 @@ class PlanInfo(ctypes.Structure):
         ("wavelet_levels", ctypes.c_int32),
         ("wavelet_coeffs", ctypes.c_int64),
         ("fft_line_width", ctypes.c_int32),
+        ("spread_columns", ctypes.c_int32),
     ]
 
 
@@ -90,6 +91,15 @@ class PdhgParams(ctypes.Structure):
 class PdhgState(ctypes.Structure):
     _fields_ = [(name, ctypes.c_void_p) for name in
                 ("u", "u_bar", "p_m", "p_ex", "p_ey", "p_ez", "p_w1", "p_w2", "w2adj", "q", "y", "g")]
+
+
+class PdhgShard(ctypes.Structure):
+    _fields_ = [
+        ("n_bins_global", ctypes.c_int32),
+        ("bin_offset", ctypes.c_int32),
+        ("u_bar_next", ctypes.c_void_p),
+        ("p_m_prev", ctypes.c_void_p),
+    ]
 
 
 _lock = threading.Lock()
@@ -130,6 +140,8 @@ def load() -> ctypes.CDLL:
             "tr_conv3d_fwd": ([vp, vp, vp, vp, i32, i32, i32, i32, i32, i32, vp], i32),
             "tr_conv3d_wgrad_workspace": ([i32, i32, i32, i32, i32, i32, ctypes.POINTER(ctypes.c_size_t)], i32),
             "tr_conv3d_wgrad": ([vp, vp, vp, i32, i32, i32, i32, i32, i32, vp, ctypes.c_size_t, vp], i32),
+            "tr_pdhg_phase": ([vp, ctypes.POINTER(PdhgState), ctypes.POINTER(PdhgParams), ctypes.POINTER(PdhgShard),
+                               i32, vp, vp], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(lib, name)

@@ -74,6 +74,17 @@ __device__ __forceinline__ void tma_store_3d(const void* tmap, const void* src, 
                  ::"l"(tmap), "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
                  : "memory");
 }
+__device__ __forceinline__ void tma_store_4d(const void* tmap, const void* src, int c0, int c1, int c2, int c3) {
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4, %5}], [%1];\n"
+                 ::"l"(tmap), "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+                 : "memory");
+}
+// contiguous global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
 // generic-proxy shared-memory writes -> visible to the TMA (async proxy)
 __device__ __forceinline__ void fence_proxy_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -95,21 +106,21 @@ template <>
 struct Dft<2> {
     __device__ __forceinline__ static void run(float2 (&v)[2], bool) {
         float2 a = v[0], b = v[1];
-        v[0] = cadd(a, b);
-        v[1] = csub(a, b);
+        v[0] = cadd_p(a, b);
+        v[1] = csub_p(a, b);
     }
 };
 
 template <>
 struct Dft<4> {
     __device__ __forceinline__ static void run(float2 (&v)[4], bool inv) {
-        float2 s0 = cadd(v[0], v[2]), d0 = csub(v[0], v[2]);
-        float2 s1 = cadd(v[1], v[3]), d1 = csub(v[1], v[3]);
+        float2 s0 = cadd_p(v[0], v[2]), d0 = csub_p(v[0], v[2]);
+        float2 s1 = cadd_p(v[1], v[3]), d1 = csub_p(v[1], v[3]);
         float2 rd1 = inv ? mul_pi(d1) : mul_mi(d1);
-        v[0] = cadd(s0, s1);
-        v[2] = csub(s0, s1);
-        v[1] = cadd(d0, rd1);
-        v[3] = csub(d0, rd1);
+        v[0] = cadd_p(s0, s1);
+        v[2] = csub_p(s0, s1);
+        v[1] = cadd_p(d0, rd1);
+        v[3] = csub_p(d0, rd1);
     }
 };
 
@@ -120,8 +131,8 @@ struct Dft<8> {
         float2 a[4], b[4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            a[r] = cadd(v[r], v[r + 4]);
-            b[r] = csub(v[r], v[r + 4]);
+            a[r] = cadd_p(v[r], v[r + 4]);
+            b[r] = csub_p(v[r], v[r + 4]);
         }
         // b_r *= w_8^r  (forward w_8 = (1 - i)/sqrt2)
         if (!inv) {
@@ -180,13 +191,13 @@ struct DftOdd {
         float2 s[H + 1], d[H + 1];
 #pragma unroll
         for (int r = 1; r <= H; ++r) {
-            s[r] = cadd(v[r], v[R - r]);
-            d[r] = csub(v[r], v[R - r]);
+            s[r] = cadd_p(v[r], v[R - r]);
+            d[r] = csub_p(v[r], v[R - r]);
         }
         float2 out[R];
         float2 x0 = v[0];
 #pragma unroll
-        for (int r = 1; r <= H; ++r) x0 = cadd(x0, s[r]);
+        for (int r = 1; r <= H; ++r) x0 = cadd_p(x0, s[r]);
         out[0] = x0;
 #pragma unroll
         for (int m = 1; m <= H; ++m) {
@@ -198,12 +209,12 @@ struct DftOdd {
                 float sg = 1.f;
                 if (k > H) { k = R - k; sg = -1.f; }
                 float cv = OddTables<R>::c(k), sv = sg * OddTables<R>::s(k);
-                re = make_float2(re.x + cv * s[r].x, re.y + cv * s[r].y);
-                im = make_float2(im.x + sv * d[r].x, im.y + sv * d[r].y);
+                re = cfma_real(cv, s[r], re);
+                im = cfma_real(sv, d[r], im);
             }
             float2 t = inv ? mul_pi(im) : mul_mi(im);
-            out[m] = cadd(re, t);
-            out[R - m] = csub(re, t);
+            out[m] = cadd_p(re, t);
+            out[R - m] = csub_p(re, t);
         }
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = out[r];
@@ -234,7 +245,7 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, int L, 
             if (r > 0 && k > 0) {
                 float2 t = tw[k * r * step];
                 if (inv) t.y = -t.y;
-                x = cmul(x, t);
+                x = cmul_p(x, t);
             }
             v[r] = x;
         }
@@ -312,7 +323,7 @@ struct CtStage {
                     if (Ns > 1 && r > 0) {
                         float2 t = tw[k * r * STEP];
                         if (INV) t.y = -t.y;
-                        x = cmul(x, t);
+                        x = cmul_p(x, t);
                     }
                     v[r] = x;
                 }

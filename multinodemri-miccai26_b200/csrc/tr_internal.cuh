@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -42,20 +43,60 @@ __host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return mak
 __host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-// c + w * v on both components with one packed f32x2 FMA (sm_100); the same
-// single rounding per component as two scalar FMAs.
+// Packed f32x2 complex arithmetic (sm_100 add/sub/mul/fma.rn.f32x2): each
+// instruction rounds both components exactly like the scalar operation, so
+// results match scalar IEEE code op for op; host builds use the scalar forms.
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+__device__ __forceinline__ unsigned long long f2_pack(float2 a) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2_unpack(unsigned long long r) {
+    float2 d;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(r));
+    return d;
+}
+#endif
+// a + b
+__device__ __forceinline__ float2 cadd_p(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_pack(a)), "l"(f2_pack(b)));
+    return f2_unpack(r);
+#else
+    return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+// a - b
+__device__ __forceinline__ float2 csub_p(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_pack(a)), "l"(f2_pack(b)));
+    return f2_unpack(r);
+#else
+    return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
+// c + w * v (real w on both components)
 __device__ __forceinline__ float2 cfma_real(float w, float2 v, float2 c) {
 #if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
-    unsigned long long rw, rv, rc, rd;
-    asm("mov.b64 %0, {%1, %1};" : "=l"(rw) : "f"(w));
-    asm("mov.b64 %0, {%1, %2};" : "=l"(rv) : "f"(v.x), "f"(v.y));
-    asm("mov.b64 %0, {%1, %2};" : "=l"(rc) : "f"(c.x), "f"(c.y));
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(rd) : "l"(rw), "l"(rv), "l"(rc));
-    float2 d;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(rd));
-    return d;
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(f2_pack(make_float2(w, w))), "l"(f2_pack(v)), "l"(f2_pack(c)));
+    return f2_unpack(r);
 #else
     return make_float2(fmaf(w, v.x, c.x), fmaf(w, v.y, c.y));
+#endif
+}
+// a * b as a.x * (b.x, b.y) + a.y * (-b.y, b.x): one packed multiply, one packed FMA
+__device__ __forceinline__ float2 cmul_p(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    unsigned long long t, r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(t) : "l"(f2_pack(make_float2(a.y, a.y))), "l"(f2_pack(make_float2(-b.y, b.x))));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(f2_pack(make_float2(a.x, a.x))), "l"(f2_pack(b)), "l"(t));
+    return f2_unpack(r);
+#else
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 #endif
 }
 // a * conj(b)
@@ -156,7 +197,10 @@ struct tr_plan {
     int* err_host = nullptr;     // pinned copy, refreshed with the tolerance scalars
     // launch shapes
     int line_width = 16;
-    bool use_tma = true;         // TMA-tiled FFT passes where the geometry allows
+    int spread_cols = 128;       // most k-space columns per gridding CTA
+    bool use_tma = true;
+    bool autotune = false;       // TR_PLAN_AUTOTUNE: time launch-shape candidates on first use
+    std::map<int, int> spread_cols_tuned;   // column count -> chosen spread_cols         // TMA-tiled FFT passes where the geometry allows
     // TVMW
     tr::WaveletPlan* wav = nullptr;
     // CUDA graph of one PDHG iteration

@@ -969,7 +969,8 @@ __global__ void __launch_bounds__(256) k_interp(const float2* __restrict__ grid,
 // k_spread_reduce then adds the partial tiles to the grid in range order.
 constexpr int kTile = 4;
 constexpr int kSpreadSub = 64;      // list entries staged per sub-chunk
-constexpr int kZeroTiles = 4;       // empty tiles per zero-fill CTA
+constexpr int kZeroTiles = 4;       // empty tiles per zero-fill CTA (plain stores)
+constexpr int kZeroTilesTma = 16;   // empty tiles per zero-fill CTA (TMA stores)
 constexpr int kSplitEntries = 256;  // longest list range of one work item
 
 struct SpreadArgs {
@@ -981,6 +982,7 @@ struct SpreadArgs {
     const int4* work;          // bin base [n_work]: (tile, first entry, end entry, partial slot or -1)
     int n_busy, n_empty, n_work;
     float2* partials;          // [slot][64 points][ncol] partial tiles of split lists
+    int* err;                  // device error word (kDevErr* bits)
     const float2* vals;        // (M_b, ncol) bin base
     int ncol, cchunk;          // columns per CTA (blockIdx.y selects the chunk)
     int use_dcf;
@@ -1008,35 +1010,61 @@ __device__ __forceinline__ void tile_geometry(const SpreadArgs& a, int tile, int
     Tx = min(kTile, a.os2 - t0x);
 }
 
-template <int CG>
-__global__ void __launch_bounds__(256, (CG >= 6 ? 3 : 4)) k_spread(SpreadArgs a) {
-    extern __shared__ __align__(16) unsigned char smraw[];
+// Tile gather.  TMA = true (even column counts, aligned k-space): each
+// entry's values arrive by one bulk copy (cp.async.bulk) on an mbarrier, the
+// dcf weight folds into the row weights, and finished tiles (and the zero
+// tiles) leave by one 4-D TMA store each, clipped at the grid edge by the TMA
+// unit.  TMA = false: values staged by plain loads, coalesced warp stores.
+template <int CG, bool TMA>
+__global__ void __launch_bounds__(256, (CG >= 6 ? 3 : (CG >= 4 ? 4 : 5))) k_spread(SpreadArgs a,
+                                                                 const __grid_constant__ CUtensorMap tgrid) {
+    extern __shared__ __align__(128) unsigned char smraw_[];
     __shared__ int l_rel[kSpreadSub];
+    __shared__ float s_dcf[kSpreadSub];
     __shared__ float s_wzy[kSpreadSub * 16];
     __shared__ __align__(16) float s_wx[kSpreadSub * 4];
+    __shared__ __align__(8) uint64_t bar;
+    unsigned char* smraw = reinterpret_cast<unsigned char*>(align128(smraw_));
     float* c_w = reinterpret_cast<float*>(smraw);                        // [kSpreadSub][16]
-    float2* dq = reinterpret_cast<float2*>(c_w + 16 * kSpreadSub);       // [kSpreadSub][ncc]
+    float2* dq = reinterpret_cast<float2*>(c_w + 16 * kSpreadSub);       // [kSpreadSub][cchunk]
     const int tid = threadIdx.x;
+    const int cst = a.cchunk;                                            // row stride of dq
 
     if ((int)blockIdx.x >= a.n_work) {
         // ---- zero fill of tiles that no sample reaches (all columns, chunk 0 only)
         if (blockIdx.y != 0) return;
-        const int warp = tid >> 5, lane = tid & 31;
-        const int z0 = ((int)blockIdx.x - a.n_work) * kZeroTiles;
-        for (int r = warp; r < kZeroTiles * 16; r += 8) {
-            const int zi = z0 + (r >> 4);
-            if (zi >= a.n_empty) break;
-            int t0z, t0y, t0x, Tz, Ty, Tx;
-            tile_geometry(a, a.tile_order[a.n_busy + zi], t0z, t0y, t0x, Tz, Ty, Tx);
-            const int pz = (r >> 2) & 3, py = r & 3;
-            if (pz >= Tz || py >= Ty) continue;
-            float2* dst = a.grid + (((int64_t)(t0z + pz) * a.os1 + (t0y + py)) * a.os2 + t0x) * a.ncol;
-            const int n2 = Tx * a.ncol;
-            if ((reinterpret_cast<uintptr_t>(dst) & 15) == 0 && (n2 & 1) == 0) {
-                float4* d4 = reinterpret_cast<float4*>(dst);
-                for (int i = lane; i < (n2 >> 1); i += 32) d4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            } else {
-                for (int i = lane; i < n2; i += 32) dst[i] = make_float2(0.f, 0.f);
+        const int zper = TMA ? kZeroTilesTma : kZeroTiles;
+        const int z0 = ((int)blockIdx.x - a.n_work) * zper;
+        if constexpr (TMA) {
+            float4* z4 = reinterpret_cast<float4*>(dq);
+            for (int i = tid; i < 32 * cst; i += 256) z4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            fence_proxy_async_smem();
+            __syncthreads();
+            if (tid == 0) {
+                for (int zi = z0; zi < min(z0 + zper, a.n_empty); ++zi) {
+                    int t0z, t0y, t0x, Tz, Ty, Tx;
+                    tile_geometry(a, a.tile_order[a.n_busy + zi], t0z, t0y, t0x, Tz, Ty, Tx);
+                    for (int c0 = 0; c0 < a.ncol; c0 += cst) tma_store_4d(&tgrid, dq, c0, t0x, t0y, t0z);
+                }
+                tma_store_commit_and_drain();
+            }
+        } else {
+            const int warp = tid >> 5, lane = tid & 31;
+            for (int r = warp; r < zper * 16; r += 8) {
+                const int zi = z0 + (r >> 4);
+                if (zi >= a.n_empty) break;
+                int t0z, t0y, t0x, Tz, Ty, Tx;
+                tile_geometry(a, a.tile_order[a.n_busy + zi], t0z, t0y, t0x, Tz, Ty, Tx);
+                const int pz = (r >> 2) & 3, py = r & 3;
+                if (pz >= Tz || py >= Ty) continue;
+                float2* dst = a.grid + (((int64_t)(t0z + pz) * a.os1 + (t0y + py)) * a.os2 + t0x) * a.ncol;
+                const int n2 = Tx * a.ncol;
+                if ((reinterpret_cast<uintptr_t>(dst) & 15) == 0 && (n2 & 1) == 0) {
+                    float4* d4 = reinterpret_cast<float4*>(dst);
+                    for (int i = lane; i < (n2 >> 1); i += 32) d4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+                } else {
+                    for (int i = lane; i < n2; i += 32) dst[i] = make_float2(0.f, 0.f);
+                }
             }
         }
         return;
@@ -1048,6 +1076,7 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : 4)) k_spread(SpreadArgs a)
     const int tile = item.x, beg = item.y, end = item.z, slot = item.w;
     int t0z, t0y, t0x, Tz, Ty, Tx;
     tile_geometry(a, tile, t0z, t0y, t0x, Tz, Ty, Tx);
+    if (TMA && tid == 0) mbar_init(&bar, 1);
 
     const int row = tid >> 4;          // tile row (z, y) = (row / 4, row % 4)
     const int g = tid & 15;
@@ -1058,23 +1087,41 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : 4)) k_spread(SpreadArgs a)
 #pragma unroll
         for (int j = 0; j < CG; ++j) acc[x][j] = make_float2(0.f, 0.f);
 
-    for (int base = beg; base < end; base += kSpreadSub) {
+    unsigned phase = 0;
+    for (int base = beg; base < end; base += kSpreadSub, phase ^= 1u) {
         const int ns = min(kSpreadSub, end - base);
+        if constexpr (TMA) {
+            __syncthreads();                       // dq free; the barrier init is visible
+            if (tid < 32) {                        // warp 0: one bulk copy per entry
+                if (tid == 0) mbar_expect_tx(&bar, (unsigned)(ns * ncc * sizeof(float2)));
+                __syncwarp();
+                for (int cand = tid; cand < ns; cand += 32) {
+                    const int sm = a.list[base + cand].x;
+                    bulk_g2s(dq + cand * cst, a.vals + (int64_t)sm * a.ncol + col0, (unsigned)(ncc * sizeof(float2)),
+                             &bar);
+                }
+            }
+        }
         if (tid < 4 * ns) {
             const int cand = tid >> 2, part = tid & 3;
             const int2 e = a.list[base + cand];
             reinterpret_cast<float4*>(c_w)[cand * 4 + part] = a.taps[e.x].w[part];
-            if (part == 0) l_rel[cand] = e.y;
+            if (part == 0) {
+                l_rel[cand] = e.y;
+                s_dcf[cand] = (TMA && a.use_dcf) ? a.ks[e.x].w : 1.0f;
+            }
         }
-        for (int cand = tid >> 5; cand < ns; cand += 8) {     // one warp per entry, lanes over columns
-            const int sm = a.list[base + cand].x;
-            const float2* src = a.vals + (int64_t)sm * a.ncol + col0;
-            const float dw = a.use_dcf ? a.ks[sm].w : 1.0f;
-            for (int col = tid & 31; col < ncc; col += 32) dq[cand * ncc + col] = cscale(src[col], dw);
+        if constexpr (!TMA) {
+            for (int cand = tid >> 5; cand < ns; cand += 8) {     // one warp per entry, lanes over columns
+                const int sm = a.list[base + cand].x;
+                const float2* src = a.vals + (int64_t)sm * a.ncol + col0;
+                const float dw = a.use_dcf ? a.ks[sm].w : 1.0f;
+                for (int col = tid & 31; col < ncc; col += 32) dq[cand * cst + col] = cscale(src[col], dw);
+            }
         }
         __syncthreads();
-        // per entry: the (z, y) weight of each of the 16 tile rows and the x weight
-        // of each of the 4 tile columns (zero where the support misses the tile)
+        // per entry: the (z, y) weight of each of the 16 tile rows (times the dcf
+        // weight on the TMA path) and the x weight of each of the 4 tile columns
         for (int i = tid; i < ns * 20; i += 256) {
             const int cand = i / 20, k = i - cand * 20;
             const int pk = l_rel[cand];
@@ -1082,13 +1129,22 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : 4)) k_spread(SpreadArgs a)
             if (k < 16) {
                 const int az = (pk & 0xff) - 128 + (k >> 2);
                 const int ay = ((pk >> 8) & 0xff) - 128 + (k & 3);
-                s_wzy[cand * 16 + k] = ((unsigned)az <= 4u && (unsigned)ay <= 4u) ? w[az] * w[5 + ay] : 0.f;
+                s_wzy[cand * 16 + k] =
+                    ((unsigned)az <= 4u && (unsigned)ay <= 4u) ? (w[az] * w[5 + ay]) * s_dcf[cand] : 0.f;
             } else {
                 const int ax = ((pk >> 16) & 0xff) - 128 + (k - 16);
                 s_wx[cand * 4 + (k - 16)] = (unsigned)ax <= 4u ? w[10 + ax] : 0.f;
             }
         }
-        __syncthreads();
+        if constexpr (TMA) {
+            const bool ok = mbar_wait_bounded(&bar, phase, kMbarPollLimit);
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) atomicOr(a.err, kDevErrTmaWait);
+                return;
+            }
+        } else {
+            __syncthreads();
+        }
         for (int cc = 0; cc < ns; ++cc) {
             const float wzy = s_wzy[cc * 16 + row];
             if (wzy == 0.f) continue;
@@ -1096,7 +1152,7 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : 4)) k_spread(SpreadArgs a)
             const float wx[4] = {wx4.x, wx4.y, wx4.z, wx4.w};
             float2 v[CG];
 #pragma unroll
-            for (int j = 0; j < CG; ++j) v[j] = (c_lo + j < ncc) ? dq[cc * ncc + c_lo + j] : make_float2(0.f, 0.f);
+            for (int j = 0; j < CG; ++j) v[j] = (c_lo + j < ncc) ? dq[cc * cst + c_lo + j] : make_float2(0.f, 0.f);
 #pragma unroll
             for (int x = 0; x < 4; ++x) {
                 if (wx[x] == 0.f) continue;
@@ -1105,21 +1161,31 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : 4)) k_spread(SpreadArgs a)
                 for (int j = 0; j < CG; ++j) acc[x][j] = cfma_real(wt, v[j], acc[x][j]);
             }
         }
-        __syncthreads();
+        if constexpr (!TMA) __syncthreads();
     }
-    // ---- stage the tile as [64 points][ncc] in shared memory (the value buffer
-    // holds kSpreadSub * ncc >= 64 * ncc), then store it coalesced, one warp per
-    // point; a split list's partial tile goes to its slot instead of the grid
+    // ---- stage the tile as [64 points][cchunk] in shared memory (the value buffer
+    // holds kSpreadSub * cchunk >= 64 * cchunk), then store it: one TMA box, or
+    // coalesced warp stores (one warp per point); a split list's partial tile
+    // goes to its slot instead of the grid
     static_assert(kSpreadSub >= 64, "the value buffer must hold a whole tile");
     __syncthreads();
 #pragma unroll
     for (int x = 0; x < 4; ++x)
 #pragma unroll
         for (int j = 0; j < CG; ++j)
-            if (c_lo + j < ncc) dq[(row * 4 + x) * ncc + c_lo + j] = acc[x][j];
+            if (c_lo + j < ncc) dq[(row * 4 + x) * cst + c_lo + j] = acc[x][j];
+    if (TMA && slot < 0) {
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            tma_store_4d(&tgrid, dq, col0, t0x, t0y, t0z);
+            tma_store_commit_and_drain();
+        }
+        return;
+    }
     __syncthreads();
     const int warp = tid >> 5, lane = tid & 31;
-    const bool vec = ((ncc | a.ncol | col0) & 1) == 0;
+    const bool vec = ((ncc | a.ncol | col0 | cst) & 1) == 0;
     for (int pt = warp; pt < 64; pt += 8) {
         const int qz = pt >> 4, qy = (pt >> 2) & 3, qx = pt & 3;
         float2* dst;
@@ -1129,7 +1195,7 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : 4)) k_spread(SpreadArgs a)
             if (qz >= Tz || qy >= Ty || qx >= Tx) continue;
             dst = a.grid + (((int64_t)(t0z + qz) * a.os1 + (t0y + qy)) * a.os2 + (t0x + qx)) * a.ncol + col0;
         }
-        const float2* src = dq + pt * ncc;
+        const float2* src = dq + pt * cst;
         if (vec) {
             for (int c = lane; c < (ncc >> 1); c += 32)
                 reinterpret_cast<float4*>(dst)[c] = reinterpret_cast<const float4*>(src)[c];
@@ -1467,12 +1533,16 @@ static tr_status stage_interp(tr_plan* p, int bin, int ncol, int mode, float sig
     return TR_OK;
 }
 
-template <int CG>
-static tr_status launch_spread_t(const SpreadArgs& sa, unsigned ntiles, unsigned nchunks, cudaStream_t st) {
-    const size_t smem = (size_t)kSpreadSub * 16 * sizeof(float) + (size_t)kSpreadSub * sa.cchunk * sizeof(float2);
-    TR_TRY(set_smem_limit((const void*)k_spread<CG>, smem));
-    k_spread<CG><<<dim3(ntiles, nchunks), 256, smem, st>>>(sa);
-    TR_CHECK_LAUNCH();
+template <int CG, bool TMA>
+static tr_status launch_spread_t(const SpreadArgs& sa, const CUtensorMap& tgrid, unsigned nx, unsigned nchunks,
+                                 cudaStream_t st) {
+    const size_t smem = (size_t)kSpreadSub * 16 * sizeof(float) + (size_t)kSpreadSub * sa.cchunk * sizeof(float2) + 128;
+    const void* fn = (const void*)k_spread<CG, TMA>;
+    TR_TRY(set_smem_limit(fn, smem));
+    SpreadArgs args_copy = sa;
+    CUtensorMap map_copy = tgrid;
+    void* args[] = {&args_copy, &map_copy};
+    TR_CUDA(cudaLaunchKernel(fn, dim3(nx, nchunks), dim3(256), args, smem, st));
     return TR_OK;
 }
 
@@ -1492,8 +1562,9 @@ static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, 
     sa.partials = p->bufB;     // free during gridding (the adjoint z pass fills it afterwards)
     sa.vals = ksp;
     sa.ncol = ncol;
-    const int nch = (ncol + 127) / 128;
+    const int nch = (ncol + p->spread_cols - 1) / p->spread_cols;
     sa.cchunk = (ncol + nch - 1) / nch;
+    if (nch > 1 && (sa.cchunk & 1)) ++sa.cchunk;     // even chunks keep TMA boxes aligned
     sa.use_dcf = (use_dcf && p->has_dcf) ? 1 : 0;
     sa.grid = p->bufA;
     sa.os0 = p->os[0];
@@ -1501,13 +1572,35 @@ static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, 
     sa.os2 = p->os[2];
     sa.nt1 = p->ntile[1];
     sa.nt2 = p->ntile[2];
+    sa.err = p->dev_err;
     const int cg = (sa.cchunk + 15) / 16;
-    const unsigned nx = (unsigned)(sa.n_work + (sa.n_empty + kZeroTiles - 1) / kZeroTiles);
-    if (cg <= 1) TR_TRY(launch_spread_t<1>(sa, nx, nch, st));
-    else if (cg <= 2) TR_TRY(launch_spread_t<2>(sa, nx, nch, st));
-    else if (cg <= 4) TR_TRY(launch_spread_t<4>(sa, nx, nch, st));
-    else if (cg <= 6) TR_TRY(launch_spread_t<6>(sa, nx, nch, st));
-    else TR_TRY(launch_spread_t<8>(sa, nx, nch, st));
+    // TMA path: even column counts and chunks, 16-byte aligned k-space rows, an encodable grid map
+    CUtensorMap tgrid;
+    std::memset(&tgrid, 0, sizeof(tgrid));
+    bool tma = p->use_tma && (ncol % 2) == 0 && (sa.cchunk % 2) == 0 && ((uintptr_t)ksp % 16) == 0;
+    if (tma) {
+        PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+        const cuuint64_t dims[4] = {(cuuint64_t)ncol, (cuuint64_t)p->os[2], (cuuint64_t)p->os[1], (cuuint64_t)p->os[0]};
+        const cuuint64_t strides[3] = {(cuuint64_t)ncol * 8, (cuuint64_t)ncol * 8 * p->os[2],
+                                       (cuuint64_t)ncol * 8 * p->os[2] * p->os[1]};
+        const cuuint32_t box[4] = {(cuuint32_t)sa.cchunk, kTile, kTile, kTile};
+        const cuuint32_t estr[4] = {1, 1, 1, 1};
+        tma = enc && enc(&tgrid, CU_TENSOR_MAP_DATA_TYPE_INT64, 4, p->bufA, dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    }
+    const int zper = tma ? kZeroTilesTma : kZeroTiles;
+    const unsigned nx = (unsigned)(sa.n_work + (sa.n_empty + zper - 1) / zper);
+#define TR_SPREAD_CG(CGV)                                                    \
+    TR_TRY((tma ? launch_spread_t<CGV, true>(sa, tgrid, nx, nch, st)         \
+                : launch_spread_t<CGV, false>(sa, tgrid, nx, nch, st)))
+    if (cg <= 1) TR_SPREAD_CG(1);
+    else if (cg <= 2) TR_SPREAD_CG(2);
+    else if (cg <= 3) TR_SPREAD_CG(3);
+    else if (cg <= 4) TR_SPREAD_CG(4);
+    else if (cg <= 6) TR_SPREAD_CG(6);
+    else TR_SPREAD_CG(8);
+#undef TR_SPREAD_CG
     if (b.n_split > 0) {
         k_spread_reduce<<<(unsigned)b.n_split, 256, 0, st>>>(sa, p->splits + b.split_offset);
         TR_CHECK_LAUNCH();
@@ -1618,10 +1711,60 @@ tr_status nufft_forward_cols(tr_plan* p, int bin, const float2* images, int64_t 
     return stage_interp(p, bin, ncol, mode, sigma, y, out, st);
 }
 
+// Launch-shape autotuning (TR_PLAN_AUTOTUNE).  The first gridding of a column
+// count, outside stream capture, times k_spread for each candidate column chunk
+// on the caller's bin (CUDA events, best of two launches after one warm-up) and
+// keeps the fastest for that column count.  The choice cannot change results:
+// every grid point sums its list in the same order whatever the chunking.
+static tr_status tune_spread_cols(tr_plan* p, int bin, const float2* ksp, int ncol, bool use_dcf, cudaStream_t st) {
+    auto it = p->spread_cols_tuned.find(ncol);
+    if (it != p->spread_cols_tuned.end()) {
+        p->spread_cols = it->second;
+        return TR_OK;
+    }
+    p->spread_cols = 128;
+    if (!p->autotune || ncol <= 16) return TR_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    TR_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return TR_OK;
+    cudaEvent_t e0, e1;
+    TR_CUDA(cudaEventCreate(&e0));
+    TR_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int best_cols = 128, last_chunk = -1;
+    tr_status rc = TR_OK;
+    for (int cols : {32, 48, 64, 96, 128}) {
+        const int nch = (ncol + cols - 1) / cols;
+        const int chunk = (ncol + nch - 1) / nch;
+        if (chunk == last_chunk) continue;       // same launch shape as the previous candidate
+        last_chunk = chunk;
+        p->spread_cols = cols;
+        rc = stage_spread(p, bin, ksp, ncol, use_dcf, st);
+        if (rc != TR_OK) break;
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 2 && rc == TR_OK; ++r) rc = stage_spread(p, bin, ksp, ncol, use_dcf, st);
+        cudaEventRecord(e1, st);
+        if (rc != TR_OK || cudaEventSynchronize(e1) != cudaSuccess) break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) {
+            best = ms;
+            best_cols = cols;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    TR_TRY(rc);
+    p->spread_cols = best_cols;
+    p->spread_cols_tuned[ncol] = best_cols;
+    return TR_OK;
+}
+
 tr_status nufft_adjoint_cols(tr_plan* p, int bin, const float2* ksp, int n_img, const float2* maps, int C,
                              bool use_dcf, float2* images, int64_t img_stride, cudaStream_t st) {
     const int ncol = n_img * C;
     TR_TRY(ensure_nufft_buffers(p, (size_t)ncol));
+    TR_TRY(tune_spread_cols(p, bin, ksp, ncol, use_dcf, st));
     TR_TRY(stage_spread(p, bin, ksp, ncol, use_dcf, st));
     TR_TRY(stage_adj_z(p, ncol, st));
     TR_TRY(stage_adj_y(p, ncol, st));
@@ -1647,6 +1790,7 @@ tr_status profile_nufft(tr_plan* p, int bin, int reps, double* ms, double* bytes
     cudaMemsetAsync(img, 0, (size_t)E * N * sizeof(float2), st);
     cudaMemsetAsync(ksp, 0, (size_t)std::max<int64_t>(M, 1) * ncol * sizeof(float2), st);
     cudaMemsetAsync(yk, 0, (size_t)std::max<int64_t>(M, 1) * ncol * sizeof(float2), st);
+    TR_TRY(tune_spread_cols(p, bin, ksp, ncol, true, st));
     bytes[0] = c8 * (E * N + C * N + XP * ncol);
     bytes[1] = c8 * ncol * (XP + YP);
     bytes[2] = c8 * ncol * (YP + G);
@@ -2013,6 +2157,7 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
     TR_CUDA(cudaMemset(p->dev_err, 0, sizeof(int)));
     *p->err_host = 0;
     p->use_tma = (d->flags & TR_PLAN_NO_TMA) == 0;
+    p->autotune = (d->flags & TR_PLAN_AUTOTUNE) != 0;
     p->workspace_bytes = (int64_t)(nks * (sizeof(float4) + sizeof(TapRec) + sizeof(int32_t)) +
                                    glist.size() * sizeof(int2) + (gwork.size() + gsplits.size()) * sizeof(int4) +
                                    (lstart.size() + torder.size()) * sizeof(int32_t));
@@ -2049,6 +2194,7 @@ tr_status tr_plan_info(const tr_plan* p, tr_plan_info_t* info) {
     info->total_samples = p->total;
     info->workspace_bytes = p->workspace_bytes;
     info->fft_line_width = p->line_width;
+    info->spread_columns = p->spread_cols;
     info->wavelet_levels = 0;
     info->wavelet_coeffs = 0;
     wavelet_info(p, &info->wavelet_levels, &info->wavelet_coeffs);

@@ -54,6 +54,9 @@ struct PdArgs {
     float2* pw1;
     int alg, l2;
     int B, E, Z, Y, X;
+    int Bg, b0;                 // bins of the whole problem; global index of local bin 0
+    const float2* ubar_next;    // (E, N) u_bar of global bin b0 + B (another rank's), or null
+    const float2* pm_prev;      // (E, N) p_m of global bin b0 - 1 (another rank's), or null
     int64_t N;
     float sigma, tau, lam_m, lam_e, lam_w1;
     double* partials;
@@ -75,7 +78,8 @@ __global__ void __launch_bounds__(256) k_dual(PdArgs a) {
     const int x = rem - y * a.X;
     const int64_t EN = (int64_t)a.E * a.N;
     const float2* ub = a.ubar + (int64_t)b * EN;
-    const float2* ubn = (b + 1 < a.B) ? ub + EN : nullptr;
+    // u_bar of the next global bin: local, the halo from the next rank, or none at the global end
+    const float2* ubn = (b + 1 < a.B) ? ub + EN : ((a.b0 + b + 1 < a.Bg) ? a.ubar_next : nullptr);
     const float sig = a.sigma;
     float s2 = 0.f;
     for (int e = 0; e < a.E; ++e) {
@@ -192,19 +196,23 @@ __global__ void __launch_bounds__(256) k_primal(PdArgs a) {
         const int x = rem - y * a.X;
         const int64_t EN = (int64_t)a.E * a.N;
         const float tau = a.tau;
+        const int gb = a.b0 + b;              // global bin
         float2 divprev = make_float2(0.f, 0.f);
         for (int e = 0; e < a.E; ++e) {
             const int64_t o = (int64_t)b * EN + (int64_t)e * a.N + v;
             const float2 uo = a.u[o];
             const float2 g = a.g[o];
+            // p_m of the previous global bin: local, or the halo from the previous rank
+            float2 pprev = make_float2(0.f, 0.f);
+            if (gb > 0) pprev = (b > 0) ? a.pm[o - EN] : a.pm_prev[(int64_t)e * a.N + v];
             float2 un;
             if (a.alg == TR_ALG_TVME) {
                 // divp_m = D_m^T p_m  (tvme.py:421-437)
                 float2 dm = make_float2(0.f, 0.f);
-                if (a.B > 1) {
-                    if (b == 0) dm = make_float2(-a.pm[o].x, -a.pm[o].y);
-                    else if (b == a.B - 1) dm = a.pm[o - EN];
-                    else dm = csub(a.pm[o - EN], a.pm[o]);
+                if (a.Bg > 1) {
+                    if (gb == 0) dm = make_float2(-a.pm[o].x, -a.pm[o].y);
+                    else if (gb == a.Bg - 1) dm = pprev;
+                    else dm = csub(pprev, a.pm[o]);
                 }
                 // divp = dxb(p_ex) + dyb(p_ey) + dzb(p_ez) at (b, e)
                 const float2 dx = back_diff(a.pex + (o - v), v, 1, x, a.X);
@@ -223,15 +231,15 @@ __global__ void __launch_bounds__(256) k_primal(PdArgs a) {
             } else if (a.alg == TR_ALG_TVM) {
                 // divergence = p[b] - p[b-1] with the reference's edges (tvm.py:342-357)
                 float2 dv;
-                if (a.B == 1) dv = make_float2(0.f, 0.f);
-                else if (b == 0) dv = a.pm[o];
-                else if (b == a.B - 1) dv = make_float2(-a.pm[o - EN].x, -a.pm[o - EN].y);
-                else dv = csub(a.pm[o], a.pm[o - EN]);
+                if (a.Bg == 1) dv = make_float2(0.f, 0.f);
+                else if (gb == 0) dv = a.pm[o];
+                else if (gb == a.Bg - 1) dv = make_float2(-pprev.x, -pprev.y);
+                else dv = csub(a.pm[o], pprev);
                 const float2 r = csub(g, dv);
                 un = make_float2(uo.x + (-tau) * r.x, uo.y + (-tau) * r.y);
             } else {
                 // TVMW: u_tmp -= tau (g - divp_m + divp_w1 + divp_w2)  (tvmw.py:662-681)
-                float2 dvm = (b == 0) ? a.pm[o] : csub(a.pm[o], a.pm[o - EN]);
+                float2 dvm = (gb == 0) ? a.pm[o] : csub(a.pm[o], pprev);
                 const float s = 0.70710678118654752f;
                 float2 w1;
                 if ((e & 1) == 0) {
@@ -301,11 +309,54 @@ static tr_status validate(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_para
     return TR_OK;
 }
 
-static tr_status enqueue_iteration(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_params* q, cudaStream_t st) {
+// Local bins [0, B) of the plan sit at global bins [b0, b0 + B) of Bg; the
+// halos carry the neighbouring ranks' edge bins (null where this plan holds the
+// global first / last bin).
+struct ShardView {
+    int Bg = 0, b0 = 0;
+    const float2* ubar_next = nullptr;
+    const float2* pm_prev = nullptr;
+};
+
+static PdArgs make_args(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_params* q, const ShardView& sh) {
+    PdArgs a;
+    memset(&a, 0, sizeof(a));
+    a.ubar = (const float2*)s->u_bar;
+    a.u = (float2*)s->u;
+    a.ubar_out = (float2*)s->u_bar;
+    a.g = (const float2*)s->g;
+    a.w2adj = (const float2*)s->w2adj;
+    a.pm = (float2*)s->p_m;
+    a.pex = (float2*)s->p_ex;
+    a.pey = (float2*)s->p_ey;
+    a.pez = (float2*)s->p_ez;
+    a.pw1 = (float2*)s->p_w1;
+    a.alg = q->algorithm;
+    a.l2 = q->l2_coupling;
+    a.B = p->B;
+    a.E = p->E;
+    a.Z = p->n[0];
+    a.Y = p->n[1];
+    a.X = p->n[2];
+    a.Bg = sh.Bg > 0 ? sh.Bg : p->B;
+    a.b0 = sh.b0;
+    a.ubar_next = sh.ubar_next;
+    a.pm_prev = sh.pm_prev;
+    a.N = (int64_t)p->n[0] * p->n[1] * p->n[2];
+    a.sigma = q->sigma;
+    a.tau = q->tau;
+    a.lam_m = q->lam_m;
+    a.lam_e = q->lam_e;
+    a.lam_w1 = q->lam_w1;
+    return a;
+}
+
+// Phase 1: every dual update and the data gradient (reads u_bar, u_bar_next).
+static tr_status enqueue_phase1(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_params* q, const ShardView& sh,
+                                cudaStream_t st) {
     const int64_t N = (int64_t)p->n[0] * p->n[1] * p->n[2];
     const int64_t EN = (int64_t)p->E * N;
     const int ncol = p->E * p->C;
-    float2* u = (float2*)s->u;
     float2* ubar = (float2*)s->u_bar;
     float2* qd = (float2*)s->q;
     const float2* y = (const float2*)s->y;
@@ -320,33 +371,8 @@ static tr_status enqueue_iteration(tr_plan* p, const tr_pdhg_state* s, const tr_
                                   y + off, qd + off, st));
     }
     // 2. TV / W1 duals
-    PdArgs a;
-    memset(&a, 0, sizeof(a));
-    a.ubar = ubar;
-    a.u = u;
-    a.ubar_out = ubar;
-    a.g = g;
-    a.w2adj = (const float2*)s->w2adj;
-    a.pm = (float2*)s->p_m;
-    a.pex = (float2*)s->p_ex;
-    a.pey = (float2*)s->p_ey;
-    a.pez = (float2*)s->p_ez;
-    a.pw1 = (float2*)s->p_w1;
-    a.alg = q->algorithm;
-    a.l2 = q->l2_coupling;
-    a.B = p->B;
-    a.E = p->E;
-    a.Z = p->n[0];
-    a.Y = p->n[1];
-    a.X = p->n[2];
-    a.N = N;
-    a.sigma = q->sigma;
-    a.tau = q->tau;
-    a.lam_m = q->lam_m;
-    a.lam_e = q->lam_e;
-    a.lam_w1 = q->lam_w1;
-    const int64_t nthr = (int64_t)p->B * N;
-    const unsigned blocks = (unsigned)((nthr + 255) / 256);
+    PdArgs a = make_args(p, s, q, sh);
+    const unsigned blocks = (unsigned)(((int64_t)p->B * N + 255) / 256);
     k_dual<<<blocks, 256, 0, st>>>(a);
     TR_CHECK_LAUNCH();
     // 3. coil-combined, density-weighted adjoint
@@ -355,18 +381,34 @@ static tr_status enqueue_iteration(tr_plan* p, const tr_pdhg_state* s, const tr_
         TR_TRY(nufft_adjoint_cols(p, b, qd + off, p->E, p->maps, p->C, true, g + (int64_t)b * EN, N, st));
     }
     if (q->algorithm == TR_ALG_TVMW) TR_TRY(wavelet_adjoint(p, (const float2*)s->p_w2, (float2*)s->w2adj, st));
-    // 4. primal, extrapolation, tolerance partials
+    return TR_OK;
+}
+
+// Phase 2: primal update, extrapolation and the FP64 tolerance sums of the
+// local bins into sums_out[2] (device memory); reads p_m and p_m_prev.
+static tr_status enqueue_phase2(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_params* q, const ShardView& sh,
+                                double* sums_out, cudaStream_t st) {
+    const int64_t N = (int64_t)p->n[0] * p->n[1] * p->n[2];
+    const unsigned blocks = (unsigned)(((int64_t)p->B * N + 255) / 256);
     if (!p->partials || p->npartials < (int)blocks) {
         cudaFree(p->partials);
         p->partials = nullptr;
         TR_CUDA(cudaMalloc(&p->partials, (size_t)blocks * 2 * sizeof(double)));
         p->npartials = (int)blocks;
     }
+    PdArgs a = make_args(p, s, q, sh);
     a.partials = p->partials;
     k_primal<<<blocks, 256, 0, st>>>(a);
     TR_CHECK_LAUNCH();
-    k_tol_finalize<<<1, 256, 0, st>>>(p->partials, (int)blocks, p->tol_dev);
+    k_tol_finalize<<<1, 256, 0, st>>>(p->partials, (int)blocks, sums_out);
     TR_CHECK_LAUNCH();
+    return TR_OK;
+}
+
+static tr_status enqueue_iteration(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_params* q, cudaStream_t st) {
+    const ShardView whole;
+    TR_TRY(enqueue_phase1(p, s, q, whole, st));
+    TR_TRY(enqueue_phase2(p, s, q, whole, p->tol_dev, st));
     TR_CUDA(cudaMemcpyAsync(p->tol_host, p->tol_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
     TR_CUDA(cudaMemcpyAsync(p->err_host, p->dev_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     return TR_OK;
@@ -461,6 +503,49 @@ extern "C" tr_status tr_pdhg_run(tr_plan* plan, const tr_pdhg_state* state, cons
     if (iters_done) *iters_done = done;
     if (prev >= 0 && prev != plan->device) cudaSetDevice(prev);
     return s;
+}
+
+extern "C" tr_status tr_pdhg_phase(tr_plan* plan, const tr_pdhg_state* state, const tr_pdhg_params* params,
+                                   const tr_pdhg_shard* shard, int32_t phase, double* tol_sums, void* stream) {
+    if (!plan || !shard) return fail(TR_ERR_INVALID_ARG, "tr_pdhg_phase: null argument");
+    TR_TRY(validate(plan, state, params));
+    if (phase != 1 && phase != 2) return fail(TR_ERR_INVALID_ARG, "tr_pdhg_phase: phase must be 1 or 2");
+    if (shard->bin_offset < 0 || shard->n_bins_global < shard->bin_offset + plan->B)
+        return fail(TR_ERR_INVALID_ARG, "tr_pdhg_phase: n_bins_global must cover bin_offset + the plan's bins");
+    const bool has_next = shard->bin_offset + plan->B < shard->n_bins_global;
+    const bool has_prev = shard->bin_offset > 0;
+    if (phase == 1 && has_next && !shard->u_bar_next)
+        return fail(TR_ERR_INVALID_ARG, "tr_pdhg_phase: u_bar_next is required unless the plan holds the last bin");
+    if (phase == 2 && has_prev && !shard->p_m_prev)
+        return fail(TR_ERR_INVALID_ARG, "tr_pdhg_phase: p_m_prev is required unless the plan holds the first bin");
+    if (phase == 2 && !tol_sums) return fail(TR_ERR_INVALID_ARG, "tr_pdhg_phase: tol_sums is required in phase 2");
+    if (*plan->err_host != 0) {
+        const int bits = *plan->err_host;
+        *plan->err_host = 0;
+        cudaMemsetAsync(plan->dev_err, 0, sizeof(int), (cudaStream_t)stream);
+        return fail(TR_ERR_TIMEOUT, "a bounded device wait expired in an earlier phase (error bits " +
+                                        std::to_string(bits) + "); results are invalid");
+    }
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != plan->device) cudaSetDevice(plan->device);
+    ShardView sh;
+    sh.Bg = shard->n_bins_global;
+    sh.b0 = shard->bin_offset;
+    sh.ubar_next = has_next ? (const float2*)shard->u_bar_next : nullptr;
+    sh.pm_prev = has_prev ? (const float2*)shard->p_m_prev : nullptr;
+    cudaStream_t st = (cudaStream_t)stream;
+    tr_status rc;
+    if (phase == 1) {
+        rc = enqueue_phase1(plan, state, params, sh, st);
+    } else {
+        rc = enqueue_phase2(plan, state, params, sh, tol_sums, st);
+        if (rc == TR_OK && cudaMemcpyAsync(plan->err_host, plan->dev_err, sizeof(int), cudaMemcpyDeviceToHost, st) !=
+                               cudaSuccess)
+            rc = fail(TR_ERR_CUDA, "tr_pdhg_phase: error-word copy failed");
+    }
+    if (prev >= 0 && prev != plan->device) cudaSetDevice(prev);
+    return rc;
 }
 
 // ------------------------------------------------------------------ FP64 diagnostics

@@ -211,6 +211,7 @@ class B200NufftBackend(NufftBackend):
         info = _lib.PlanInfo()
         _lib.check(lib.tr_plan_info(self._plan, ctypes.byref(info)))
         self.os_shape = tuple(info.os_shape)
+        self.autotune = bool(autotune)
         self.total_samples = int(info.total_samples)
         self.wavelet_levels = int(info.wavelet_levels)
         self.wavelet_coeffs = int(info.wavelet_coeffs)
@@ -344,6 +345,13 @@ class B200NufftBackend(NufftBackend):
         self._torch.cuda.synchronize(self.device)
         return {name: {"ms": ms[i], "bytes": by[i], "gbs": by[i] / (ms[i] * 1e6) if ms[i] > 0 else 0.0}
                 for i, name in enumerate(self.STAGES)}
+
+    @property
+    def spread_columns(self) -> int:
+        """k-space columns per gridding CTA (the autotuner's choice once it has run)."""
+        info = _lib.PlanInfo()
+        _lib.check(self._lib.tr_plan_info(self._plan, ctypes.byref(info)))
+        return int(info.spread_columns)
 
     def close(self) -> None:
         if getattr(self, "_plan", None):

@@ -38,6 +38,7 @@ def main(argv=None):
     ap.add_argument("--pdhg", type=int, default=0, help="also run this many TVME iterations (all bins)")
     ap.add_argument("--bins", type=int, default=2)
     ap.add_argument("--no-tma", action="store_true", help="stage the FFT passes with cp.async instead of TMA")
+    ap.add_argument("--autotune", action="store_true", help="let the plan time its launch-shape candidates")
     args = ap.parse_args(argv)
     import torch
     syn = importlib.import_module(f"{PKG}.synthetic")
@@ -47,13 +48,13 @@ def main(argv=None):
     coord = syn.cones_trajectory(shape, args.cones, args.readout, rng).reshape(-1, 3)
     dcf = syn.density(coord, shape)
     be = nb.B200NufftBackend(shape, [coord], 0, dcf=[dcf], n_coils=args.coils, n_echoes=args.echoes,
-                             tma=not args.no_tma)
+                             tma=not args.no_tma, autotune=args.autotune)
     mps = syn.coil_maps(shape, args.coils, rng)
     be.set_maps(mps)
     prof = be.profile(0, reps=args.reps)
     torch.cuda.synchronize()
-    out = {"tma": not args.no_tma, "shape_zyx": list(shape), "os_shape": list(be.os_shape), "coils": args.coils, "echoes": args.echoes,
-           "samples": int(coord.shape[0]), "stages": {k: {kk: round(vv, 4) for kk, vv in v.items()}
+    out = {"tma": not args.no_tma, "spread_columns": be.spread_columns, "shape_zyx": list(shape),
+           "os_shape": list(be.os_shape), "coils": args.coils, "echoes": args.echoes, "samples": int(coord.shape[0]), "stages": {k: {kk: round(vv, 4) for kk, vv in v.items()}
                                                       for k, v in prof.items()}}
     be.close()
     if args.pdhg:

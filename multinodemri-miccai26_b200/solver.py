@@ -41,7 +41,7 @@ class PdhgSolver:
     def __init__(self, algorithm: str, img_shape: Sequence[int], coords, dcf, mps, ksp, *, device=0,
                  l2_coupling: bool = False, sigma: float = 1 / 6, tau: float = 1 / 6, lam_m: float = 1e-5,
                  lam_e: float = 1e-5, lam_w1: float = 1e-5, lam_w2: float = 1e-5, use_graph: bool = True,
-                 backend: Optional[B200NufftBackend] = None):
+                 backend: Optional[B200NufftBackend] = None, autotune: bool = True):
         import torch
         self.torch = torch
         self.algorithm = algorithm.lower()
@@ -54,7 +54,7 @@ class PdhgSolver:
         self.E = int(first.shape[0])
         self.B = len(ksp)
         self.backend = backend or B200NufftBackend(self.img_shape, coords, device, dcf=dcf, n_coils=self.C,
-                                                   n_echoes=self.E)
+                                                   n_echoes=self.E, autotune=autotune)
         self.device = self.backend.device
         self.stream = torch.cuda.Stream(self.device)
         self.l2_coupling = bool(l2_coupling)
