@@ -968,7 +968,9 @@ __global__ void __launch_bounds__(256) k_interp(const float2* __restrict__ grid,
 // trailing CTAs write zeros into tiles no sample reaches, kZeroTiles each.
 // k_spread_reduce then adds the partial tiles to the grid in range order.
 constexpr int kTile = 4;
-constexpr int kSpreadSub = 64;      // list entries staged per sub-chunk
+constexpr int kSpreadSub = 32;      // list entries staged per sub-chunk (= points of two z planes of a tile)
+constexpr int kSlabZ = kSpreadSub / 16;            // z planes per staged piece of a finished tile
+static_assert(kSpreadSub % 16 == 0 && 64 % kSpreadSub == 0, "pieces of whole z planes");
 constexpr int kZeroTiles = 4;       // empty tiles per zero-fill CTA (plain stores)
 constexpr int kZeroTilesTma = 16;   // empty tiles per zero-fill CTA (TMA stores)
 constexpr int kSplitEntries = 256;  // longest list range of one work item
@@ -1036,15 +1038,16 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : (CG >= 4 ? 4 : 5))) k_spre
         const int zper = TMA ? kZeroTilesTma : kZeroTiles;
         const int z0 = ((int)blockIdx.x - a.n_work) * zper;
         if constexpr (TMA) {
-            float4* z4 = reinterpret_cast<float4*>(dq);
-            for (int i = tid; i < 32 * cst; i += 256) z4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            float4* z4 = reinterpret_cast<float4*>(dq);          // one zero piece [kSpreadSub][cchunk]
+            for (int i = tid; i < (kSpreadSub / 2) * cst; i += 256) z4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
             fence_proxy_async_smem();
             __syncthreads();
             if (tid == 0) {
                 for (int zi = z0; zi < min(z0 + zper, a.n_empty); ++zi) {
                     int t0z, t0y, t0x, Tz, Ty, Tx;
                     tile_geometry(a, a.tile_order[a.n_busy + zi], t0z, t0y, t0x, Tz, Ty, Tx);
-                    for (int c0 = 0; c0 < a.ncol; c0 += cst) tma_store_4d(&tgrid, dq, c0, t0x, t0y, t0z);
+                    for (int c0 = 0; c0 < a.ncol; c0 += cst)
+                        for (int hz = 0; hz < kTile; hz += kSlabZ) tma_store_4d(&tgrid, dq, c0, t0x, t0y, t0z + hz);
                 }
                 tma_store_commit_and_drain();
             }
@@ -1163,44 +1166,49 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : (CG >= 4 ? 4 : 5))) k_spre
         }
         if constexpr (!TMA) __syncthreads();
     }
-    // ---- stage the tile as [64 points][cchunk] in shared memory (the value buffer
-    // holds kSpreadSub * cchunk >= 64 * cchunk), then store it: one TMA box, or
-    // coalesced warp stores (one warp per point); a split list's partial tile
+    // ---- store the tile in pieces of kSlabZ z planes: each piece is staged as
+    // [kSpreadSub points][cchunk] in the value buffer, then leaves as one TMA box,
+    // or by coalesced warp stores (one warp per point); a split list's partial tile
     // goes to its slot instead of the grid
-    static_assert(kSpreadSub >= 64, "the value buffer must hold a whole tile");
-    __syncthreads();
-#pragma unroll
-    for (int x = 0; x < 4; ++x)
-#pragma unroll
-        for (int j = 0; j < CG; ++j)
-            if (c_lo + j < ncc) dq[(row * 4 + x) * cst + c_lo + j] = acc[x][j];
-    if (TMA && slot < 0) {
-        fence_proxy_async_smem();
-        __syncthreads();
-        if (tid == 0) {
-            tma_store_4d(&tgrid, dq, col0, t0x, t0y, t0z);
-            tma_store_commit_and_drain();
-        }
-        return;
-    }
-    __syncthreads();
+    constexpr int kPieceRows = kSpreadSub / 4;            // tile rows (z, y) per piece
     const int warp = tid >> 5, lane = tid & 31;
     const bool vec = ((ncc | a.ncol | col0 | cst) & 1) == 0;
-    for (int pt = warp; pt < 64; pt += 8) {
-        const int qz = pt >> 4, qy = (pt >> 2) & 3, qx = pt & 3;
-        float2* dst;
-        if (slot >= 0) {
-            dst = a.partials + ((int64_t)slot * 64 + pt) * a.ncol + col0;
-        } else {
-            if (qz >= Tz || qy >= Ty || qx >= Tx) continue;
-            dst = a.grid + (((int64_t)(t0z + qz) * a.os1 + (t0y + qy)) * a.os2 + (t0x + qx)) * a.ncol + col0;
+    for (int piece = 0; piece < 64 / kSpreadSub; ++piece) {
+        __syncthreads();                                   // dq free (values, or the previous piece)
+        if (row / kPieceRows == piece) {
+#pragma unroll
+            for (int x = 0; x < 4; ++x)
+#pragma unroll
+                for (int j = 0; j < CG; ++j)
+                    if (c_lo + j < ncc) dq[((row % kPieceRows) * 4 + x) * cst + c_lo + j] = acc[x][j];
         }
-        const float2* src = dq + pt * cst;
-        if (vec) {
-            for (int c = lane; c < (ncc >> 1); c += 32)
-                reinterpret_cast<float4*>(dst)[c] = reinterpret_cast<const float4*>(src)[c];
-        } else {
-            for (int c = lane; c < ncc; c += 32) dst[c] = src[c];
+        if (TMA && slot < 0) {
+            fence_proxy_async_smem();
+            __syncthreads();
+            if (tid == 0) {
+                tma_store_4d(&tgrid, dq, col0, t0x, t0y, t0z + kSlabZ * piece);
+                tma_store_commit_and_drain();
+            }
+            continue;
+        }
+        __syncthreads();
+        for (int hp = warp; hp < kSpreadSub; hp += 8) {
+            const int pt = piece * kSpreadSub + hp;
+            const int qz = pt >> 4, qy = (pt >> 2) & 3, qx = pt & 3;
+            float2* dst;
+            if (slot >= 0) {
+                dst = a.partials + ((int64_t)slot * 64 + pt) * a.ncol + col0;
+            } else {
+                if (qz >= Tz || qy >= Ty || qx >= Tx) continue;
+                dst = a.grid + (((int64_t)(t0z + qz) * a.os1 + (t0y + qy)) * a.os2 + (t0x + qx)) * a.ncol + col0;
+            }
+            const float2* src = dq + hp * cst;
+            if (vec) {
+                for (int c = lane; c < (ncc >> 1); c += 32)
+                    reinterpret_cast<float4*>(dst)[c] = reinterpret_cast<const float4*>(src)[c];
+            } else {
+                for (int c = lane; c < ncc; c += 32) dst[c] = src[c];
+            }
         }
     }
 }
@@ -1583,7 +1591,7 @@ static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, 
         const cuuint64_t dims[4] = {(cuuint64_t)ncol, (cuuint64_t)p->os[2], (cuuint64_t)p->os[1], (cuuint64_t)p->os[0]};
         const cuuint64_t strides[3] = {(cuuint64_t)ncol * 8, (cuuint64_t)ncol * 8 * p->os[2],
                                        (cuuint64_t)ncol * 8 * p->os[2] * p->os[1]};
-        const cuuint32_t box[4] = {(cuuint32_t)sa.cchunk, kTile, kTile, kTile};
+        const cuuint32_t box[4] = {(cuuint32_t)sa.cchunk, kTile, kTile, kSlabZ};   // one staged piece
         const cuuint32_t estr[4] = {1, 1, 1, 1};
         tma = enc && enc(&tgrid, CU_TENSOR_MAP_DATA_TYPE_INT64, 4, p->bufA, dims, strides, box, estr,
                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
