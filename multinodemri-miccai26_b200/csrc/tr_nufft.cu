@@ -339,6 +339,10 @@ __global__ void __launch_bounds__(256) k_adj_x(AdjXArgs a) {
 #define TR_CT_NARROW(X) X(240) X(320)
 #define TR_CT_LENGTHS(X) TR_CT_WIDE(X) TR_CT_NARROW(X)
 __host__ __device__ constexpr int ct_width(int L) { return L >= 240 ? 8 : 16; }
+// The TMA x passes take 8 coils per CTA at every length: their rows are contiguous,
+// so narrow tiles cost no DRAM efficiency and buy occupancy (the strided y / z
+// passes keep 16-column tiles up to L = 200: 128-byte row segments).
+constexpr int kTmaXWidth = 8;
 
 template <int L, int W, bool INV>
 __global__ void __launch_bounds__(256) k_line_ct(LineArgs a) {
@@ -1448,9 +1452,9 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
     fa.out = p->bufA;
     fa.ncol = n_img * C;
     fa.err = p->dev_err;
-    // TMA variant: one image row x Wct coils per CTA
-    if (p->use_tma && ct && maps && C % Wct == 0 && X % 16 == 0 && X <= 256 && img_stride % 2 == 0 &&
-        (int64_t)X * (Wct + 1) <= (int64_t)OSX * Wct && OSX / 2 <= 256) {
+    // TMA variant: one image row x kTmaXWidth coils per CTA
+    if (p->use_tma && ct && maps && C % kTmaXWidth == 0 && X % 16 == 0 && X <= 256 && img_stride % 2 == 0 &&
+        (int64_t)X * (kTmaXWidth + 1) <= (int64_t)OSX * kTmaXWidth && OSX / 2 <= 256) {
         CUtensorMap timg, tmap, tout;
         const uint64_t nrows = (uint64_t)Z * Y;
         PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
@@ -1464,17 +1468,17 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
         }
-        ok = ok && encode_map_3d(&tmap, maps, (uint64_t)C, (uint64_t)X, nrows, (uint32_t)Wct, (uint32_t)X);
-        ok = ok && encode_map_3d(&tout, p->bufA, (uint64_t)fa.ncol, (uint64_t)OSX, nrows, (uint32_t)Wct,
+        ok = ok && encode_map_3d(&tmap, maps, (uint64_t)C, (uint64_t)X, nrows, (uint32_t)kTmaXWidth, (uint32_t)X);
+        ok = ok && encode_map_3d(&tout, p->bufA, (uint64_t)fa.ncol, (uint64_t)OSX, nrows, (uint32_t)kTmaXWidth,
                                  (uint32_t)(OSX / 2));
         const void* tfn = nullptr;
-#define TR_FWDX_TMA(LV) case LV: tfn = (const void*)k_fwd_x_tma<LV, ct_width(LV)>; break;
+#define TR_FWDX_TMA(LV) case LV: tfn = (const void*)k_fwd_x_tma<LV, kTmaXWidth>; break;
         switch (OSX) { TR_CT_LENGTHS(TR_FWDX_TMA) default: break; }
 #undef TR_FWDX_TMA
         if (ok && tfn) {
-            const size_t smem = fft_smem_bytes(OSX, Wct) + 128;
+            const size_t smem = fft_smem_bytes(OSX, kTmaXWidth) + 128;
             TR_TRY(set_smem_limit(tfn, smem));
-            dim3 grid((unsigned)(nrows * n_img), 1u, (unsigned)(C / Wct));
+            dim3 grid((unsigned)(nrows * n_img), 1u, (unsigned)(C / kTmaXWidth));
             void* args[] = {&fa, &timg, &tmap, &tout};
             TR_CUDA(cudaLaunchKernel(tfn, grid, dim3(256), args, smem, st));
             return TR_OK;
@@ -1667,16 +1671,16 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
     aa.img_stride = img_stride;
     aa.accumulate = 0;
     aa.err = p->dev_err;
-    // TMA variant: one image row per CTA, coil groups of Wct
-    if (p->use_tma && ct && maps && C % Wct == 0 && OSX / 2 <= 256 && X <= 256 && X + 4 <= OSX) {
+    // TMA variant: one image row per CTA, coil groups of kTmaXWidth
+    if (p->use_tma && ct && maps && C % kTmaXWidth == 0 && OSX / 2 <= 256 && X <= 256 && X + 4 <= OSX) {
         CUtensorMap tin;
         const void* tfn = nullptr;
-#define TR_ADJX_TMA(LV) case LV: tfn = (const void*)k_adj_x_tma<LV, ct_width(LV)>; break;
+#define TR_ADJX_TMA(LV) case LV: tfn = (const void*)k_adj_x_tma<LV, kTmaXWidth>; break;
         switch (OSX) { TR_CT_LENGTHS(TR_ADJX_TMA) default: break; }
 #undef TR_ADJX_TMA
-        if (tfn && encode_map_3d(&tin, p->bufA, (uint64_t)aa.ncol, (uint64_t)OSX, (uint64_t)Z * Y, (uint32_t)Wct,
+        if (tfn && encode_map_3d(&tin, p->bufA, (uint64_t)aa.ncol, (uint64_t)OSX, (uint64_t)Z * Y, (uint32_t)kTmaXWidth,
                                  (uint32_t)(OSX / 2))) {
-            const size_t smem = fft_smem_bytes(OSX, Wct) + 128;
+            const size_t smem = fft_smem_bytes(OSX, kTmaXWidth) + 128;
             TR_TRY(set_smem_limit(tfn, smem));
             dim3 grid((unsigned)((int64_t)Z * Y * n_img));
             void* args[] = {&aa, &tin};
