@@ -55,6 +55,17 @@ METRIC = "TVME time-to-tol 1e-3 (s) on 1 B200, warm-start vs plain PDHG; NUFFT G
 FALLBACK_HBM_GBS = 6650.0
 WARM_MATCH = 1e-3      # warm-started result must match the plain result to this relative L2
 
+# DRAM bytes (read + write) of one launch of each NUFFT stage, from ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) on one bin of this trajectory
+# and grid with 16 k-space columns (profiles/nufft_pdhg_kernels_256x256x128_16col.md);
+# the grid-sized traffic scales with the column count, so roofline.traffic for the
+# 96-column bench workload is these figures x ncol / 16.
+NCU_TRAFFIC_16COL = {
+    "workload": "tvme-256", "columns": 16,
+    "fwd_x": 1.962e9, "fwd_y": 2.974e9, "fwd_z": 3.723e9, "interp": 1.303e9,
+    "spread": 2.296e9, "adj_z": 3.732e9, "adj_y": 2.984e9, "adj_x": 2.012e9,
+}
+
 # Iterations to --tol of plain PDHG on each seeded workload, measured with the
 # b200 arm on the same seeded problem; the CPU reference arm cannot run a full
 # solve within minutes and extrapolates its per-iteration time with these.
@@ -246,7 +257,9 @@ def run_b200(args):
     st = solver.stream
     E, C, B = solver.E, solver.C, solver.B
     ncol = E * C
-    launches_per_iter = B * (4 + math.ceil(ncol / 128) + 3) + 3
+    # per bin: x, y, z passes + interpolation; gridding + split-tile reduction + z, y, x passes;
+    # per iteration: TV duals, primal, tolerance reduction
+    launches_per_iter = B * (4 + math.ceil(ncol / 128) + 1 + 3) + 3
     if cfg.algorithm == "tvmw":
         launches_per_iter += 6 * max(1, solver.backend.wavelet_levels)
 
@@ -286,6 +299,10 @@ def run_b200(args):
     dom_name = max(prof, key=lambda k: prof[k]["ms"])
     dom = prof[dom_name]
     nufft_ms = sum(v["ms"] for v in prof.values())
+    traffic, traffic_src = None, None
+    if cfg.name == NCU_TRAFFIC_16COL["workload"] and dom_name in NCU_TRAFFIC_16COL:
+        traffic = round(NCU_TRAFFIC_16COL[dom_name] * (E * C) / NCU_TRAFFIC_16COL["columns"])
+        traffic_src = f"ncu DRAM bytes at 16 columns x {E * C}/16"
     nufft_bytes = sum(v["bytes"] for v in prof.values())
 
     # ---- FP64 oracle agreement and warm/plain agreement
@@ -369,7 +386,8 @@ def run_b200(args):
                                  "frac": round(v["gbs"] / hbm, 3)} for k, v in prof.items()},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(dom["gbs"], 1), "peak": hbm,
                          "unit": "GB/s", "frac": round(dom["gbs"] / hbm, 3), "peak_source": peak_src,
-                         "traffic": None, "algorithmic_bytes": dom["bytes"]},
+                         "traffic": traffic, "traffic_source": traffic_src, "algorithmic_bytes": dom["bytes"],
+                         "launch_ms": round(dom["ms"], 4)},
             "clocks": clk,
             "e2e": e2e,
             "cpu_baseline": cpu,
