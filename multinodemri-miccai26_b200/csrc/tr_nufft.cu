@@ -2039,10 +2039,14 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
     }
     p->fwd_scale = (float)(1.0 / (std::sqrt(N) * std::pow((double)d->width, 3)));
     p->adj_scale = p->fwd_scale;
-    auto bad = [&](tr_status code, const std::string& m) {
-        plan_free(p);
-        return fail(code, m);
-    };
+    // frees the half-built plan on every early return (TR_CUDA / TR_TRY included)
+    struct PlanOwner {
+        tr_plan* p;
+        ~PlanOwner() {
+            if (p) plan_free(p);
+        }
+    } owner{p};
+    auto bad = [&](tr_status code, const std::string& m) { return fail(code, m); };
     for (int i = 0; i < 3; ++i) {
         FftAxis& A = p->ax[i];
         A.n = p->n[i];
@@ -2134,10 +2138,7 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
         const tr_status lrc = build_gather_lists(p, b, M ? &ks_sorted[(size_t)o] : nullptr, M, glist,
                                                  &lstart[(size_t)b * (p->ntiles + 1)], &torder[(size_t)b * p->ntiles],
                                                  gwork, gsplits);
-        if (lrc != TR_OK) {
-            plan_free(p);
-            return lrc;
-        }
+        if (lrc != TR_OK) return lrc;
     }
     const size_t nks = (size_t)std::max<int64_t>(off, 1);
     if (cudaMalloc(&p->ks, nks * sizeof(float4)) != cudaSuccess ||
@@ -2174,6 +2175,7 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
                                    glist.size() * sizeof(int2) + (gwork.size() + gsplits.size()) * sizeof(int4) +
                                    (lstart.size() + torder.size()) * sizeof(int32_t));
     TR_TRY(wavelet_prepare(p));
+    owner.p = nullptr;
     *out = p;
     return TR_OK;
 }
