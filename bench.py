@@ -514,7 +514,7 @@ def run_reference(args):
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": "s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(per_iter * 1e3, 1), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic", "impl": "reference",
+        "scaling": "strong", "vs_baseline": None, "dtype": "c64", "data": "synthetic", "impl": "reference",
         "config": {"workload": cfg.name, "algorithm": cfg.algorithm, "img_shape_zyx": list(cfg.img_shape),
                    "coils": cfg.n_coils, "echoes": cfg.n_echoes, "bins": cfg.n_bins, "tol": cfg.tol},
         "iterations": iters,
