@@ -23,12 +23,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "tr_fft.cuh"
@@ -2089,7 +2091,6 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
     // scale coordinates exactly as the reference (float32 multiply, then add)
     std::vector<float4> ks_sorted((size_t)std::max<int64_t>(off, 1));
     std::vector<int32_t> perm((size_t)std::max<int64_t>(off, 1));
-    std::vector<int32_t> tstart((size_t)(p->ntiles + 1));
     std::vector<int32_t> lstart((size_t)(p->ntiles + 1) * d->n_bins);
     std::vector<int32_t> torder((size_t)p->ntiles * d->n_bins);
     std::vector<int2> glist;
@@ -2099,18 +2100,30 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
         scale[i] = (float)((double)p->os[i] / (double)p->n[i]);
         shift[i] = (float)(p->os[i] / 2);
     }
-    std::vector<int32_t> key;
-    std::vector<float4> kscaled;
-    for (int b = 0; b < d->n_bins; ++b) {
+    // per bin (in parallel over host threads): scaled coordinates, stable counting
+    // sort by tile, gather lists; bins write disjoint ranges, lists are joined in bin order
+    struct BinOut {
+        tr_status rc = TR_OK;
+        std::string msg;
+        std::vector<int2> glist;
+        std::vector<int4> work, splits;
+    };
+    std::vector<BinOut> outs((size_t)d->n_bins);
+    auto do_bin = [&](int b) {
+        BinOut& out = outs[(size_t)b];
         const int64_t M = p->bins[b].count, o = p->bins[b].offset;
-        key.assign((size_t)M, 0);
-        kscaled.assign((size_t)M, make_float4(0, 0, 0, 0));
+        std::vector<int32_t> key((size_t)M, 0);
+        std::vector<float4> kscaled((size_t)M, make_float4(0, 0, 0, 0));
         for (int64_t m = 0; m < M; ++m) {
             float kc[3];
             for (int i = 0; i < 3; ++i) {
                 volatile float t = d->coords[(o + m) * 3 + i] * scale[i];
                 kc[i] = t + shift[i];
-                if (!std::isfinite(kc[i])) return bad(TR_ERR_INVALID_ARG, "coordinates must be finite");
+                if (!std::isfinite(kc[i])) {
+                    out.rc = TR_ERR_INVALID_ARG;
+                    out.msg = "coordinates must be finite";
+                    return;
+                }
             }
             const float w = d->dcf ? d->dcf[o + m] : 1.0f;
             kscaled[(size_t)m] = make_float4(kc[0], kc[1], kc[2], w);
@@ -2124,21 +2137,51 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
             key[(size_t)m] = (tcoord[0] * p->ntile[1] + tcoord[1]) * p->ntile[2] + tcoord[2];
         }
         // stable counting sort by tile
-        int32_t* ts = tstart.data();
-        std::fill(ts, ts + p->ntiles + 1, 0);
-        for (int64_t m = 0; m < M; ++m) ts[key[(size_t)m] + 1]++;
-        for (int64_t t = 0; t < p->ntiles; ++t) ts[t + 1] += ts[t];
-        std::vector<int32_t> fillp(ts, ts + p->ntiles);
+        std::vector<int32_t> ts((size_t)p->ntiles + 1, 0);
+        for (int64_t m = 0; m < M; ++m) ts[(size_t)key[(size_t)m] + 1]++;
+        for (int64_t t = 0; t < p->ntiles; ++t) ts[(size_t)t + 1] += ts[(size_t)t];
+        std::vector<int32_t> fillp(ts.begin(), ts.end() - 1);
         for (int64_t m = 0; m < M; ++m) {
-            const int32_t pos = fillp[key[(size_t)m]]++;
+            const int32_t pos = fillp[(size_t)key[(size_t)m]]++;
             perm[(size_t)(o + pos)] = (int32_t)m;
             ks_sorted[(size_t)(o + pos)] = kscaled[(size_t)m];
         }
         // gather lists: every (tile, sample) pair where the sample's KB support meets the tile
-        const tr_status lrc = build_gather_lists(p, b, M ? &ks_sorted[(size_t)o] : nullptr, M, glist,
-                                                 &lstart[(size_t)b * (p->ntiles + 1)], &torder[(size_t)b * p->ntiles],
-                                                 gwork, gsplits);
-        if (lrc != TR_OK) return lrc;
+        out.rc = build_gather_lists(p, b, M ? &ks_sorted[(size_t)o] : nullptr, M, out.glist,
+                                    &lstart[(size_t)b * (p->ntiles + 1)], &torder[(size_t)b * p->ntiles], out.work,
+                                    out.splits);
+        if (out.rc != TR_OK) out.msg = g_last_error;     // this worker thread's message
+    };
+    {
+        std::atomic<int> next_bin{0};
+        auto worker = [&]() {
+            for (int b; (b = next_bin++) < d->n_bins;) {
+                try {
+                    do_bin(b);
+                } catch (const std::exception& e) {
+                    outs[(size_t)b].rc = TR_ERR_OOM;
+                    outs[(size_t)b].msg = std::string("plan creation: ") + e.what();
+                }
+            }
+        };
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const int nthr = (int)std::min<unsigned>(hw, (unsigned)d->n_bins);
+        std::vector<std::thread> pool;
+        for (int i = 1; i < nthr; ++i) pool.emplace_back(worker);
+        worker();
+        for (auto& t : pool) t.join();
+    }
+    for (int b = 0; b < d->n_bins; ++b) {
+        BinOut& out = outs[(size_t)b];
+        if (out.rc != TR_OK) return bad(out.rc, out.msg);
+        Bin& B = p->bins[b];
+        B.list_offset = (int64_t)glist.size();
+        B.work_offset = (int64_t)gwork.size();
+        B.split_offset = (int64_t)gsplits.size();
+        glist.insert(glist.end(), out.glist.begin(), out.glist.end());
+        gwork.insert(gwork.end(), out.work.begin(), out.work.end());
+        gsplits.insert(gsplits.end(), out.splits.begin(), out.splits.end());
+        std::vector<int2>().swap(out.glist);
     }
     const size_t nks = (size_t)std::max<int64_t>(off, 1);
     if (cudaMalloc(&p->ks, nks * sizeof(float4)) != cudaSuccess ||
