@@ -84,6 +84,8 @@ def parse(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--jsense", action="store_true",
+                    help="time JSENSE coil-map estimation on the workload's first echo instead of PDHG")
     ap.add_argument("--sharded", action="store_true",
                     help="use the bin-sharded multi-GPU path even on one GPU (exercises its code on one device)")
     return ap.parse_args(argv)
@@ -527,8 +529,59 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------- JSENSE leg
+def run_jsense(args):
+    """JSENSE (SigPy application defaults: kernel 16, calibration 24, 10 x 10 CG
+    iterations) on the workload's first echo: the b200 version timed whole (wall
+    clock around a synchronised call), the CPU restatement (C/OpenMP KB loops,
+    multi-threaded FFTs) timed on one outer iteration with two CG steps per
+    sub-problem and scaled by NUFFT-pair count."""
+    import torch
+    syn = importlib.import_module(f"{PKG}.synthetic")
+    js = importlib.import_module(f"{PKG}.jsense")
+    cfg = get_config(args)
+    ds = syn.make_geometry(cfg)
+    syn.simulate_kspace_b200(ds, 0)
+    coord = ds.coord.reshape(-1, 3)
+    y0 = ds.ksp[0].reshape(cfg.n_coils, -1)
+    keep = np.all(np.abs(coord) < 12.0, axis=-1)
+    times = []
+    for i in range(max(1, args.warmup) + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        maps = js.estimate_sensitivity_maps(ds.ksp[:1], ds.coord, ds.dcf, image_shape_zyx=cfg.img_shape)
+        torch.cuda.synchronize()
+        if i >= max(1, args.warmup):
+            times.append(time.perf_counter() - t0)
+    t_gpu = statistics.median(times)
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import jsense as oj
+        from oracle import cgrid
+        t0 = time.perf_counter()
+        cgrid.build()
+        oj.jsense(y0, coord, ds.dcf.reshape(-1), max_iter=1, inner=2, nufft=cgrid.nufft,
+                  nufft_adjoint=cgrid.nufft_adjoint)
+        t_cpu_sample = time.perf_counter() - t0
+        pairs_full, pairs_sample = 10 * 2 * (10 + 2), 1 * 2 * (2 + 2)
+        cpu = {"value": round(t_cpu_sample * pairs_full / pairs_sample, 2), "unit": "s", "cores": cgrid.threads(),
+               "kind": "port", "sample": f"one outer iteration with 2 CG steps per sub-problem ({t_cpu_sample:.2f} s), "
+                                         f"x {pairs_full}/{pairs_sample} NUFFT pairs"}
+    print(json.dumps({
+        "metric": "JSENSE coil-map estimation time (s), first echo", "value": round(t_gpu, 4), "unit": "s",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup), "higher_is_better": False,
+        "dtype": "c64", "data": "synthetic",
+        "config": {"workload": cfg.name, "coils": cfg.n_coils, "img_shape_zyx": list(cfg.img_shape),
+                   "calibration_samples": int(keep.sum()), "kernel_width": 16, "calibration_width": 24,
+                   "outer_iterations": 10, "cg_iterations": 10},
+        "maps_shape": list(maps.shape), "cpu_baseline": cpu}), flush=True)
+
+
 def main(argv=None):
     args = parse(argv)
+    if args.jsense:
+        run_jsense(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -65,16 +65,21 @@ def cg(normal, rhs, x0, iters):
     return x
 
 
-def jsense(y, coord, weights, ker_width=16, calib_width=24, lamda=0.0, max_iter=10, inner=10):
-    """Maps (C, w, w, w) on the calibration grid from (C, M) k-space."""
+def jsense(y, coord, weights, ker_width=16, calib_width=24, lamda=0.0, max_iter=10, inner=10, nufft=None,
+           nufft_adjoint=None):
+    """Maps (C, w, w, w) on the calibration grid from (C, M) k-space.  ``nufft`` /
+    ``nufft_adjoint`` default to the restatement in ``oracle/nufft.py``; the timed
+    CPU baseline passes the C/OpenMP loops of ``oracle/cgrid.py``."""
     y, coord, w = calibration(np.asarray(y, np.complex128), np.asarray(coord, np.float64),
                               np.asarray(weights, np.float64), calib_width)
     shape = (calib_width,) * 3
     C = y.shape[0]
     scale = np.max(np.abs(y)) if y.size else 1.0
     y = y / (scale if scale > 0 else 1.0)
-    F = lambda im: onf.nufft(im, coord)                                  # (..., Z, Y, X) -> (..., M)
-    FH = lambda k: onf.nufft_adjoint(k, coord, shape)
+    fwd = nufft or onf.nufft
+    adj = nufft_adjoint or onf.nufft_adjoint
+    F = lambda im: fwd(im, coord)                                        # (..., Z, Y, X) -> (..., M)
+    FH = lambda k: adj(k, coord, shape)
     pad = lambda k: onf.resize_center(k, shape)
     crop = lambda im: onf.resize_center(im, (ker_width,) * 3)
     x = np.ones(shape, np.complex128)
