@@ -4,8 +4,9 @@
 
 Mirrors the reference's dispatch (``src/toporecon/cli.py:149-164``): the
 arguments after ``--`` go to the algorithm's ``main``.  Only ``reconstruct``
-belongs to the accelerated path; the reference's other sub-commands
-(inspect, resp, jsense, prepare, stitch) are not part of this backend.
+belongs to the accelerated path; of the reference's other sub-commands
+(inspect, resp, jsense, prepare, stitch) only the JSENSE estimation exists
+here, as the library function ``jsense.estimate_sensitivity_maps``.
 """
 
 from __future__ import annotations
