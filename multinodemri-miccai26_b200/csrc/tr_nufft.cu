@@ -799,15 +799,19 @@ __global__ void __launch_bounds__(256, (W >= 16 ? 3 : 4)) k_adj_x_tma(AdjXArgs a
     const int shift = a.h - a.pad;
     const float4* mrow = reinterpret_cast<const float4*>(a.maps + ((int64_t)row * X + x) * a.C);
     float2 s = make_float2(0.f, 0.f);
+    // the transform's last stage does not read buf0 when it writes buf1 (odd stage
+    // counts): the next group's tile then loads during this group's epilogue
+    constexpr bool kEarly = (ct_nstages(L) % 2) == 1;
+    auto issue = [&](int c0) {
+        mbar_expect_tx(&bar, (unsigned)(L * W * sizeof(float2)));
+        const int col = img * a.C + c0;
+        tma_load_3d(buf0, &tin, &bar, col, L / 2, row);
+        tma_load_3d(buf0 + (L / 2) * W, &tin, &bar, col, 0, row);
+    };
+    __syncthreads();                        // barrier initialised
+    if (threadIdx.x == 0) issue(0);
     int phase = 0;
     for (int c0 = 0; c0 < a.C; c0 += W, phase ^= 1) {
-        __syncthreads();                    // the previous group's readers of buf0 / ep are done
-        if (threadIdx.x == 0) {
-            mbar_expect_tx(&bar, (unsigned)(L * W * sizeof(float2)));
-            const int col = img * a.C + c0;
-            tma_load_3d(buf0, &tin, &bar, col, L / 2, row);
-            tma_load_3d(buf0 + (L / 2) * W, &tin, &bar, col, 0, row);
-        }
         // this column's W coil-map values, in flight during the transform
         float4 m2[W / 2];
         if (x < X) {
@@ -825,7 +829,8 @@ __global__ void __launch_bounds__(256, (W >= 16 ? 3 : 4)) k_adj_x_tma(AdjXArgs a
             if (o < X) ep[w * XP + o] = v;
         };
         fft_ct<L, W, 256, true>(buf0, buf1, tws, store);
-        __syncthreads();
+        __syncthreads();                    // transform done: buf0 free (odd stage counts), ep complete
+        if (kEarly && threadIdx.x == 0 && c0 + W < a.C) issue(c0 + W);
         // conj(S) product and the sum over this group's coils, in coil order
         if (x < X) {
 #pragma unroll
@@ -833,6 +838,10 @@ __global__ void __launch_bounds__(256, (W >= 16 ? 3 : 4)) k_adj_x_tma(AdjXArgs a
                 s = cadd(s, cmulc(ep[(2 * q) * XP + x], make_float2(m2[q].x, m2[q].y)));
                 s = cadd(s, cmulc(ep[(2 * q + 1) * XP + x], make_float2(m2[q].z, m2[q].w)));
             }
+        }
+        if (!kEarly) {
+            __syncthreads();                // the epilogue's reads of ep (= buf0) are done
+            if (threadIdx.x == 0 && c0 + W < a.C) issue(c0 + W);
         }
     }
     if (x < X) {
