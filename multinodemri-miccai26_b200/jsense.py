@@ -19,7 +19,7 @@ Every NUFFT runs through two b200 plans on the calibration trajectory (one with
 the coils as coil maps for the image step, one with the coils as separate
 images for the kernel step), with the density weights applied in the
 deterministic gridding; the small centred FFTs of the map parameterisation and
-the CG vector algebra are torch on the same device.  The checker is
+the CG vector algebra are torch on the same device.  The oracle is
 ``oracle/jsense.py``.
 """
 

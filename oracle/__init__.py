@@ -17,7 +17,7 @@ This package restates, on the CPU, the algorithms that the reference
   gridding loops (``oracle/kbgrid.c``), used for speed and as the CPU baseline.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py`` (its CPU-baseline
-and ``--impl reference`` legs) may import this package, and only as the checker
+and ``--impl reference`` legs) may import this package, and only as the reference side of a comparison
 or as the timed CPU baseline.  The product path never calls it.
 
 Parity status.  The reference's own tests pin nothing on this path (its unit

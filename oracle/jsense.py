@@ -16,7 +16,7 @@ calibration width 24, lambda 0, 10 outer and 10 inner iterations):
   ``inner`` conjugate-gradient steps on the normal equations, warm-started;
 * output: the maps on the calibration grid.
 
-Parity with SigPy is unpinned (no SigPy here); this is the checker of the b200
+Parity with SigPy is unpinned (no SigPy here); this is the oracle of the b200
 JSENSE (``multinodemri-miccai26_b200/jsense.py``), which must match it.
 Complex128 throughout.
 """
