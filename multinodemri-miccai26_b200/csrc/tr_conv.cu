@@ -44,18 +44,29 @@ struct ConvDims {
     int64_t V;   // N*D*H*W
 };
 
-__device__ __forceinline__ int64_t neighbour(const ConvDims& c, int64_t v, int t) {
-    // voxel v shifted by tap t, or -1 outside the zero-padded volume
+// Coordinates of a voxel, computed once per thread; neighbours then need only
+// integer adds and bounds checks.
+struct VoxelPos {
+    int64_t v;
+    int z, y, x;
+};
+
+__device__ __forceinline__ VoxelPos voxel_pos(const ConvDims& c, int64_t v) {
+    VoxelPos p;
+    p.v = v;
     int64_t r = v;
-    const int x = (int)(r % c.W);
+    p.x = (int)(r % c.W);
     r /= c.W;
-    const int y = (int)(r % c.H);
+    p.y = (int)(r % c.H);
     r /= c.H;
-    const int z = (int)(r % c.D);
-    const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-    const int zz = z + dz, yy = y + dy, xx = x + dx;
+    p.z = (int)(r % c.D);
+    return p;
+}
+
+__device__ __forceinline__ int64_t neighbour_at(const ConvDims& c, const VoxelPos& p, int dz, int dy, int dx) {
+    const int zz = p.z + dz, yy = p.y + dy, xx = p.x + dx;
     if (zz < 0 || zz >= c.D || yy < 0 || yy >= c.H || xx < 0 || xx >= c.W) return -1;
-    return v + ((int64_t)dz * c.H + dy) * c.W + dx;
+    return p.v + ((int64_t)dz * c.H + dy) * c.W + dx;
 }
 
 // Forward: 4 warps, 64 voxels per CTA, each warp 16 voxels x Cout.
@@ -72,9 +83,11 @@ __global__ void __launch_bounds__(128) k_conv3d_fwd(const __nv_bfloat16* __restr
 #pragma unroll
     for (int n = 0; n < NT; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
     const int K27 = 27 * c.Cin;
+    const VoxelPos pa = voxel_pos(c, va < c.V ? va : 0), pb = voxel_pos(c, vb < c.V ? vb : 0);
     for (int t = 0; t < 27; ++t) {
-        const int64_t na = va < c.V ? neighbour(c, va, t) : -1;
-        const int64_t nb = vb < c.V ? neighbour(c, vb, t) : -1;
+        const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+        const int64_t na = va < c.V ? neighbour_at(c, pa, dz, dy, dx) : -1;
+        const int64_t nb = vb < c.V ? neighbour_at(c, pb, dz, dy, dx) : -1;
         const __nv_bfloat16* xa = x + (na < 0 ? 0 : na * c.Cin);
         const __nv_bfloat16* xb = x + (nb < 0 ? 0 : nb * c.Cin);
         for (int ci0 = 0; ci0 < c.Cin; ci0 += 16) {
@@ -129,14 +142,30 @@ __global__ void __launch_bounds__(128) k_conv3d_wgrad(const __nv_bfloat16* __res
 #pragma unroll
     for (int n = 0; n < NT; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
     const __nv_bfloat16 zero = __float2bfloat16(0.f);
+    const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+    // this thread's four voxels k = 2tig, 2tig+1, 2tig+8, 2tig+9 of each 16-voxel step,
+    // with coordinates advanced incrementally (16 voxels per step along x, then y, z, volume)
+    VoxelPos pos[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) pos[j] = voxel_pos(c, min(vbeg + tig * 2 + (j & 1) + (j >> 1) * 8, c.V - 1));
     for (int64_t kb = vbeg; kb < vend; kb += 16) {
         int64_t nbr[4];
         bool in[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const int64_t v = kb + tig * 2 + (j & 1) + (j >> 1) * 8;   // k = 2tig, 2tig+1, 2tig+8, 2tig+9
+            const int64_t v = kb + tig * 2 + (j & 1) + (j >> 1) * 8;
             in[j] = v < vend;
-            nbr[j] = in[j] ? neighbour(c, v, t) : -1;
+            nbr[j] = in[j] ? neighbour_at(c, pos[j], dz, dy, dx) : -1;
+            // advance to v + 16
+            pos[j].v += 16;
+            pos[j].x += 16;
+            while (pos[j].x >= c.W) {
+                pos[j].x -= c.W;
+                if (++pos[j].y >= c.H) {
+                    pos[j].y = 0;
+                    if (++pos[j].z >= c.D) pos[j].z = 0;      // next volume of the batch
+                }
+            }
         }
         __nv_bfloat16 xa[4], xb[4];
 #pragma unroll
