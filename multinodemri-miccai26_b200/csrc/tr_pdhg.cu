@@ -66,103 +66,86 @@ __device__ __forceinline__ float2 cdivr(float2 v, float d) { return make_float2(
 __device__ __forceinline__ float cabsf(float2 v) { return sqrtf(v.x * v.x + v.y * v.y); }
 
 // ------------------------------------------------------------------ duals
-// Dual updates of one (bin, echo, voxel): motion p_m (the L1 prox here unless
-// l2, whose prox needs every echo), the TVME echo-spatial TV triple with its
-// isotropic prox, or the TVMW db1 echo wavelet with its prox.  Returns |p_m|^2.
-__device__ __forceinline__ float dual_one(const PdArgs& a, int b, int e, int64_t v, int z, int y, int x,
-                                          const float2* ub, const float2* ubn) {
-    const int64_t EN = (int64_t)a.E * a.N;
-    const int YX = a.Y * a.X;
-    const float sig = a.sigma;
-    const int64_t o = (int64_t)b * EN + (int64_t)e * a.N + v;
-    const float2 u0 = ub[(int64_t)e * a.N + v];
-    // motion: p_m += sigma (u_bar[b+1] - u_bar[b]) (0 at the last bin)
-    float2 dm = make_float2(0.f, 0.f);
-    if (ubn) dm = csub(ubn[(int64_t)e * a.N + v], u0);
-    float2 pm = a.pm[o];
-    pm = make_float2(pm.x + sig * dm.x, pm.y + sig * dm.y);
-    float m2 = 0.f;
-    if (!a.l2) {
-        const float den = fmaxf(1.0f, cabsf(pm) / a.lam_m);
-        pm = cdivr(pm, den);
-    } else {
-        const float m = cabsf(pm);
-        m2 = m * m;
-    }
-    a.pm[o] = pm;
-    if (a.alg == TR_ALG_TVME) {
-        float2 gx = make_float2(0.f, 0.f), gy = gx, gz = gx;
-        if (e + 1 < a.E) {
-            const float2* u_e = ub + (int64_t)e * a.N;
-            const float2* u_n = u_e + a.N;
-            const float2 d0 = csub(u_n[v], u_e[v]);
-            if (x + 1 < a.X) gx = csub(csub(u_n[v + 1], u_e[v + 1]), d0);
-            if (y + 1 < a.Y) gy = csub(csub(u_n[v + a.X], u_e[v + a.X]), d0);
-            if (z + 1 < a.Z) gz = csub(csub(u_n[v + YX], u_e[v + YX]), d0);
-        }
-        float2 px = a.pex[o], py = a.pey[o], pz = a.pez[o];
-        px = make_float2(px.x + sig * gx.x, px.y + sig * gx.y);
-        py = make_float2(py.x + sig * gy.x, py.y + sig * gy.y);
-        pz = make_float2(pz.x + sig * gz.x, pz.y + sig * gz.y);
-        const float ax = cabsf(px), ay = cabsf(py), az = cabsf(pz);
-        const float mag = sqrtf(ax * ax + ay * ay + az * az);
-        const float den = fmaxf(1.0f, mag / a.lam_e);
-        a.pex[o] = cdivr(px, den);
-        a.pey[o] = cdivr(py, den);
-        a.pez[o] = cdivr(pz, den);
-    } else if (a.alg == TR_ALG_TVMW) {
-        // db1 along echo: even e: (u_e + u_{e+1})/sqrt2 ; odd e: (u_e - u_{e-1})/sqrt2
-        const float s = 0.70710678118654752f;
-        float2 w;
-        if ((e & 1) == 0) {
-            float2 x1 = (e + 1 < a.E) ? ub[(int64_t)(e + 1) * a.N + v] : make_float2(0.f, 0.f);
-            w = cscale(cadd(u0, x1), s);
-        } else {
-            const float2 xm = ub[(int64_t)(e - 1) * a.N + v];
-            w = cscale(cadd(make_float2(-xm.x, -xm.y), u0), s);
-        }
-        float2 pw = a.pw1[o];
-        pw = make_float2(pw.x + sig * w.x, pw.y + sig * w.y);
-        if (a.lam_w1 > 0.f) {
-            const float den = fmaxf(1.0f, cabsf(pw) / a.lam_w1);
-            pw = cdivr(pw, den);
-        } else {
-            pw = make_float2(0.f, 0.f);
-        }
-        a.pw1[o] = pw;
-    }
-    return m2;
-}
-
-// L1 motion coupling: one thread per (bin, echo, voxel).  L2 coupling: one
-// thread per (bin, voxel) over every echo, then the joint prox of p_m.
 __global__ void __launch_bounds__(256) k_dual(PdArgs a) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t EN = (int64_t)a.E * a.N;
-    const int nE = a.l2 ? 1 : a.E;                 // echoes spread over threads
-    if (t >= (int64_t)a.B * nE * a.N) return;
-    const int b = (int)(t / ((int64_t)nE * a.N));
-    const int64_t r = t - (int64_t)b * nE * a.N;
-    const int e0 = a.l2 ? 0 : (int)(r / a.N);
-    const int64_t v = a.l2 ? r : r - (int64_t)e0 * a.N;
+    if (t >= (int64_t)a.B * a.N) return;
+    const int b = (int)(t / a.N);
+    const int64_t v = t - (int64_t)b * a.N;
     const int YX = a.Y * a.X;
     const int z = (int)(v / YX);
     const int rem = (int)(v - (int64_t)z * YX);
     const int y = rem / a.X;
     const int x = rem - y * a.X;
+    const int64_t EN = (int64_t)a.E * a.N;
     const float2* ub = a.ubar + (int64_t)b * EN;
     // u_bar of the next global bin: local, the halo from the next rank, or none at the global end
     const float2* ubn = (b + 1 < a.B) ? ub + EN : ((a.b0 + b + 1 < a.Bg) ? a.ubar_next : nullptr);
-    if (!a.l2) {
-        dual_one(a, b, e0, v, z, y, x, ub, ubn);
-        return;
-    }
+    const float sig = a.sigma;
     float s2 = 0.f;
-    for (int e = 0; e < a.E; ++e) s2 += dual_one(a, b, e, v, z, y, x, ub, ubn);
-    const float den = fmaxf(1.0f, sqrtf(s2) / a.lam_m);
     for (int e = 0; e < a.E; ++e) {
         const int64_t o = (int64_t)b * EN + (int64_t)e * a.N + v;
-        a.pm[o] = cdivr(a.pm[o], den);
+        const float2 u0 = ub[(int64_t)e * a.N + v];
+        // motion: p_m += sigma (u_bar[b+1] - u_bar[b]) (0 at the last bin)
+        float2 dm = make_float2(0.f, 0.f);
+        if (ubn) dm = csub(ubn[(int64_t)e * a.N + v], u0);
+        float2 pm = a.pm[o];
+        pm = make_float2(pm.x + sig * dm.x, pm.y + sig * dm.y);
+        if (!a.l2) {
+            const float den = fmaxf(1.0f, cabsf(pm) / a.lam_m);
+            pm = cdivr(pm, den);
+        } else {
+            const float m = cabsf(pm);
+            s2 += m * m;
+        }
+        a.pm[o] = pm;
+        if (a.alg == TR_ALG_TVME) {
+            float2 gx = make_float2(0.f, 0.f), gy = gx, gz = gx;
+            if (e + 1 < a.E) {
+                const float2* u_e = ub + (int64_t)e * a.N;
+                const float2* u_n = u_e + a.N;
+                const float2 d0 = csub(u_n[v], u_e[v]);
+                if (x + 1 < a.X) gx = csub(csub(u_n[v + 1], u_e[v + 1]), d0);
+                if (y + 1 < a.Y) gy = csub(csub(u_n[v + a.X], u_e[v + a.X]), d0);
+                if (z + 1 < a.Z) gz = csub(csub(u_n[v + YX], u_e[v + YX]), d0);
+            }
+            float2 px = a.pex[o], py = a.pey[o], pz = a.pez[o];
+            px = make_float2(px.x + sig * gx.x, px.y + sig * gx.y);
+            py = make_float2(py.x + sig * gy.x, py.y + sig * gy.y);
+            pz = make_float2(pz.x + sig * gz.x, pz.y + sig * gz.y);
+            const float ax = cabsf(px), ay = cabsf(py), az = cabsf(pz);
+            const float mag = sqrtf(ax * ax + ay * ay + az * az);
+            const float den = fmaxf(1.0f, mag / a.lam_e);
+            a.pex[o] = cdivr(px, den);
+            a.pey[o] = cdivr(py, den);
+            a.pez[o] = cdivr(pz, den);
+        } else if (a.alg == TR_ALG_TVMW) {
+            // db1 along echo: even e: (u_e + u_{e+1})/sqrt2 ; odd e: (u_e - u_{e-1})/sqrt2
+            const float s = 0.70710678118654752f;
+            float2 w;
+            if ((e & 1) == 0) {
+                float2 x1 = (e + 1 < a.E) ? ub[(int64_t)(e + 1) * a.N + v] : make_float2(0.f, 0.f);
+                w = cscale(cadd(u0, x1), s);
+            } else {
+                const float2 xm = ub[(int64_t)(e - 1) * a.N + v];
+                w = cscale(cadd(make_float2(-xm.x, -xm.y), u0), s);
+            }
+            float2 pw = a.pw1[o];
+            pw = make_float2(pw.x + sig * w.x, pw.y + sig * w.y);
+            if (a.lam_w1 > 0.f) {
+                const float den = fmaxf(1.0f, cabsf(pw) / a.lam_w1);
+                pw = cdivr(pw, den);
+            } else {
+                pw = make_float2(0.f, 0.f);
+            }
+            a.pw1[o] = pw;
+        }
+    }
+    if (a.l2) {
+        const float den = fmaxf(1.0f, sqrtf(s2) / a.lam_m);
+        for (int e = 0; e < a.E; ++e) {
+            const int64_t o = (int64_t)b * EN + (int64_t)e * a.N + v;
+            a.pm[o] = cdivr(a.pm[o], den);
+        }
     }
 }
 
@@ -389,8 +372,8 @@ static tr_status enqueue_phase1(tr_plan* p, const tr_pdhg_state* s, const tr_pdh
     }
     // 2. TV / W1 duals
     PdArgs a = make_args(p, s, q, sh);
-    const int64_t dual_threads = (int64_t)p->B * (q->l2_coupling ? 1 : p->E) * N;
-    k_dual<<<(unsigned)((dual_threads + 255) / 256), 256, 0, st>>>(a);
+    const unsigned blocks = (unsigned)(((int64_t)p->B * N + 255) / 256);
+    k_dual<<<blocks, 256, 0, st>>>(a);
     TR_CHECK_LAUNCH();
     // 3. coil-combined, density-weighted adjoint
     for (int b = 0; b < p->B; ++b) {

@@ -137,3 +137,29 @@ def test_batched_coil_echo_path(shape, E, C):
         gref = np.sum(cgrid.nufft_adjoint(dcf[b] * q, kb[b], shape) * np.conj(mps)[None], axis=1)
         assert onf.rel_l2(g, gref) < TOL_NUFFT
     be.close()
+
+
+def test_autotuned_gridding_gives_the_same_bits():
+    """The launch-shape autotuner only picks how many k-space columns a gridding
+    CTA takes; every grid point still sums its list in the same order."""
+    torch = _torch()
+    nb = pkg("nufft_backend")
+    syn = pkg("synthetic")
+    rng = np.random.default_rng(7)
+    shape = (48, 64, 96)
+    k = syn.cones_trajectory(shape, 120, 200, rng).reshape(-1, 3)
+    dcf = syn.density(k, shape)
+    C, E = 16, 6                                     # 96 columns: several chunkings are candidates
+    mps = syn.coil_maps(shape, C, rng)
+    ksp = (rng.standard_normal((k.shape[0], E * C)) + 1j * rng.standard_normal((k.shape[0], E * C)))
+    outs, chosen = [], []
+    for tune in (False, True):
+        be = nb.B200NufftBackend(shape, [k], 0, dcf=[dcf], n_coils=C, n_echoes=E, autotune=tune)
+        be.set_maps(mps)
+        y = torch.from_numpy(ksp.astype(np.complex64)).cuda()
+        outs.append(be.adjoint_bin(y, 0, use_dcf=True).clone())
+        chosen.append(be.spread_columns)
+        be.close()
+    torch.cuda.synchronize()
+    assert chosen[1] in (32, 48, 64, 96, 128)
+    assert torch.equal(outs[0], outs[1])
