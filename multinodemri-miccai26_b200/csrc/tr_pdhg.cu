@@ -66,7 +66,11 @@ __device__ __forceinline__ float2 cdivr(float2 v, float d) { return make_float2(
 __device__ __forceinline__ float cabsf(float2 v) { return sqrtf(v.x * v.x + v.y * v.y); }
 
 // ------------------------------------------------------------------ duals
+// EC > 0: the echo count as a compile-time constant (the echo loops unroll, so
+// every echo's loads are in flight together); EC = 0: any echo count.
+template <int EC>
 __global__ void __launch_bounds__(256) k_dual(PdArgs a) {
+    const int E = EC > 0 ? EC : a.E;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (int64_t)a.B * a.N) return;
     const int b = (int)(t / a.N);
@@ -76,13 +80,14 @@ __global__ void __launch_bounds__(256) k_dual(PdArgs a) {
     const int rem = (int)(v - (int64_t)z * YX);
     const int y = rem / a.X;
     const int x = rem - y * a.X;
-    const int64_t EN = (int64_t)a.E * a.N;
+    const int64_t EN = (int64_t)E * a.N;
     const float2* ub = a.ubar + (int64_t)b * EN;
     // u_bar of the next global bin: local, the halo from the next rank, or none at the global end
     const float2* ubn = (b + 1 < a.B) ? ub + EN : ((a.b0 + b + 1 < a.Bg) ? a.ubar_next : nullptr);
     const float sig = a.sigma;
     float s2 = 0.f;
-    for (int e = 0; e < a.E; ++e) {
+#pragma unroll (EC > 0 ? EC : 1)
+    for (int e = 0; e < E; ++e) {
         const int64_t o = (int64_t)b * EN + (int64_t)e * a.N + v;
         const float2 u0 = ub[(int64_t)e * a.N + v];
         // motion: p_m += sigma (u_bar[b+1] - u_bar[b]) (0 at the last bin)
@@ -100,7 +105,7 @@ __global__ void __launch_bounds__(256) k_dual(PdArgs a) {
         a.pm[o] = pm;
         if (a.alg == TR_ALG_TVME) {
             float2 gx = make_float2(0.f, 0.f), gy = gx, gz = gx;
-            if (e + 1 < a.E) {
+            if (e + 1 < E) {
                 const float2* u_e = ub + (int64_t)e * a.N;
                 const float2* u_n = u_e + a.N;
                 const float2 d0 = csub(u_n[v], u_e[v]);
@@ -123,7 +128,7 @@ __global__ void __launch_bounds__(256) k_dual(PdArgs a) {
             const float s = 0.70710678118654752f;
             float2 w;
             if ((e & 1) == 0) {
-                float2 x1 = (e + 1 < a.E) ? ub[(int64_t)(e + 1) * a.N + v] : make_float2(0.f, 0.f);
+                float2 x1 = (e + 1 < E) ? ub[(int64_t)(e + 1) * a.N + v] : make_float2(0.f, 0.f);
                 w = cscale(cadd(u0, x1), s);
             } else {
                 const float2 xm = ub[(int64_t)(e - 1) * a.N + v];
@@ -142,7 +147,8 @@ __global__ void __launch_bounds__(256) k_dual(PdArgs a) {
     }
     if (a.l2) {
         const float den = fmaxf(1.0f, sqrtf(s2) / a.lam_m);
-        for (int e = 0; e < a.E; ++e) {
+    #pragma unroll (EC > 0 ? EC : 1)
+    for (int e = 0; e < E; ++e) {
             const int64_t o = (int64_t)b * EN + (int64_t)e * a.N + v;
             a.pm[o] = cdivr(a.pm[o], den);
         }
@@ -373,7 +379,15 @@ static tr_status enqueue_phase1(tr_plan* p, const tr_pdhg_state* s, const tr_pdh
     // 2. TV / W1 duals
     PdArgs a = make_args(p, s, q, sh);
     const unsigned blocks = (unsigned)(((int64_t)p->B * N + 255) / 256);
-    k_dual<<<blocks, 256, 0, st>>>(a);
+    switch (p->E) {
+        case 1: k_dual<1><<<blocks, 256, 0, st>>>(a); break;
+        case 2: k_dual<2><<<blocks, 256, 0, st>>>(a); break;
+        case 3: k_dual<3><<<blocks, 256, 0, st>>>(a); break;
+        case 4: k_dual<4><<<blocks, 256, 0, st>>>(a); break;
+        case 6: k_dual<6><<<blocks, 256, 0, st>>>(a); break;
+        case 8: k_dual<8><<<blocks, 256, 0, st>>>(a); break;
+        default: k_dual<0><<<blocks, 256, 0, st>>>(a); break;
+    }
     TR_CHECK_LAUNCH();
     // 3. coil-combined, density-weighted adjoint
     for (int b = 0; b < p->B; ++b) {
