@@ -346,6 +346,22 @@ __host__ __device__ constexpr int ct_width(int L) { return L >= 240 ? 8 : 16; }
 // passes keep 16-column tiles up to L = 200: 128-byte row segments).
 constexpr int kTmaXWidth = 8;
 
+// Threads per CTA of the TMA line passes and the adjoint x pass: 320 for
+// 8-column tiles whose Stockham stages then run in fewer rounds, else 256.  At
+// L = 320, W = 8 the radix-8 stages have 320 butterflies: 256 threads need two
+// rounds for them (the second a quarter full), 320 threads one; measured on the
+// 160x320x320 grid with 96 columns, the y passes gain 3-4 % and the adjoint x
+// pass 1 %.  The 16-column z passes (L = 160) and the forward x pass measured
+// slower with 320 threads and keep 256.
+__host__ __device__ constexpr int ct_rounds(int L, int W, int NT) {
+    int n = 0;
+    for (int s = 0; s < ct_nstages(L); ++s) n += ((L / ct_radix(L, s)) * W + NT - 1) / NT;
+    return n;
+}
+__host__ __device__ constexpr int ct_threads(int L, int W) {
+    return (W <= 8 && ct_rounds(L, W, 320) < ct_rounds(L, W, 256)) ? 320 : 256;
+}
+
 template <int L, int W, bool INV>
 __global__ void __launch_bounds__(256) k_line_ct(LineArgs a) {
     extern __shared__ float2 sm[];
@@ -412,8 +428,8 @@ __global__ void __launch_bounds__(256) k_line_ct(LineArgs a) {
 // Lout/2 rows leave by TMA stores (rows o = (k + h - p_out) mod L < Lout).
 // One thread issues every copy; the rest of the CTA only runs the transform.
 // The load wait is bounded: on expiry the CTA sets kDevErrTmaWait and exits.
-template <int L, int W, bool INV>
-__global__ void __launch_bounds__(256) k_line_tma(LineArgs a, const __grid_constant__ CUtensorMap tin,
+template <int L, int W, bool INV, int NT = ct_threads(L, W)>
+__global__ void __launch_bounds__(NT) k_line_tma(LineArgs a, const __grid_constant__ CUtensorMap tin,
                                                   const __grid_constant__ CUtensorMap tout) {
     extern __shared__ __align__(128) unsigned char tsm_raw[];
     __shared__ __align__(8) uint64_t bar;
@@ -431,7 +447,7 @@ __global__ void __launch_bounds__(256) k_line_tma(LineArgs a, const __grid_const
         tma_load_3d(smA, &tin, &bar, q0, L / 2 - a.p_in, outer);
         tma_load_3d(smA + (L / 2) * W, &tin, &bar, q0, -a.p_in, outer);
     }
-    for (int i = threadIdx.x; i < L; i += 256) tws[i] = a.tw[i];
+    for (int i = threadIdx.x; i < L; i += NT) tws[i] = a.tw[i];
     const bool ok = mbar_wait_bounded(&bar, 0, kMbarPollLimit);
     if (__syncthreads_or(!ok)) {          // every thread leaves together
         if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
@@ -439,7 +455,7 @@ __global__ void __launch_bounds__(256) k_line_tma(LineArgs a, const __grid_const
     }
     float2* ep = fft_ct_free<L>(smA, smB);
     auto store = [ep](int k, int w, float2 v) { ep[k * W + w] = v; };
-    fft_ct<L, W, 256, INV>(smA, smB, tws, store);
+    fft_ct<L, W, NT, INV>(smA, smB, tws, store);
     fence_proxy_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -723,8 +739,8 @@ __device__ __forceinline__ float2* align128(unsigned char* p) {
     return reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(p) + 127) & ~uintptr_t(127));
 }
 
-template <int L, int W>
-__global__ void __launch_bounds__(256) k_fwd_x_tma(FwdXArgs a, const __grid_constant__ CUtensorMap timg,
+template <int L, int W, int NT = 256>
+__global__ void __launch_bounds__(NT) k_fwd_x_tma(FwdXArgs a, const __grid_constant__ CUtensorMap timg,
                                                    const __grid_constant__ CUtensorMap tmap,
                                                    const __grid_constant__ CUtensorMap tout) {
     extern __shared__ __align__(128) unsigned char xsm_raw[];
@@ -749,7 +765,7 @@ __global__ void __launch_bounds__(256) k_fwd_x_tma(FwdXArgs a, const __grid_cons
         const int z = row / a.Y, y = row - z * a.Y;
         s_apzy = a.apz[z] * a.apy[y] * a.scale;
     }
-    for (int i = threadIdx.x; i < L; i += 256) tws[i] = a.tw[i];
+    for (int i = threadIdx.x; i < L; i += NT) tws[i] = a.tw[i];
     const bool ok = mbar_wait_bounded(&bar, 0, kMbarPollLimit);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
@@ -757,7 +773,7 @@ __global__ void __launch_bounds__(256) k_fwd_x_tma(FwdXArgs a, const __grid_cons
     }
     const float apzy = s_apzy;
 #pragma unroll 4
-    for (int idx = threadIdx.x; idx < L * W; idx += 256) {
+    for (int idx = threadIdx.x; idx < L * W; idx += NT) {
         const int m = idx / W, w = idx - m * W;
         int j = m + a.h;
         if (j >= L) j -= L;
@@ -769,7 +785,7 @@ __global__ void __launch_bounds__(256) k_fwd_x_tma(FwdXArgs a, const __grid_cons
     __syncthreads();
     float2* ep = fft_ct_free<L>(smA, smB);
     auto store = [ep](int k, int w, float2 v) { ep[k * W + w] = v; };
-    fft_ct<L, W, 256, false>(smA, smB, tws, store);
+    fft_ct<L, W, NT, false>(smA, smB, tws, store);
     fence_proxy_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -780,21 +796,22 @@ __global__ void __launch_bounds__(256) k_fwd_x_tma(FwdXArgs a, const __grid_cons
     }
 }
 
-template <int L, int W>
-__global__ void __launch_bounds__(256, (W >= 16 ? 3 : 4)) k_adj_x_tma(AdjXArgs a, const __grid_constant__ CUtensorMap tin) {
+template <int L, int W, int NT = ct_threads(L, W)>
+__global__ void __launch_bounds__(NT, (W >= 16 || NT > 256 ? 3 : 4)) k_adj_x_tma(AdjXArgs a,
+                                                                                const __grid_constant__ CUtensorMap tin) {
     extern __shared__ __align__(128) unsigned char xsm_raw[];
     __shared__ __align__(8) uint64_t bar;
     float2* sm = align128(xsm_raw);
     float2* buf0 = sm;
     float2* buf1 = sm + L * W;
     float2* tws = sm + 2 * L * W;
-    const int X = a.X;                      // <= 256: thread x owns image column x
+    const int X = a.X;                      // <= 256 <= NT: thread x owns image column x
     const int XP = X + 4;                   // padded row of the [W][XP] epilogue tile
     const int img = (int)(blockIdx.x % (unsigned)a.n_img);
     const int row = (int)(blockIdx.x / (unsigned)a.n_img);
     const int x = threadIdx.x;
     if (threadIdx.x == 0) mbar_init(&bar, 1);
-    for (int i = threadIdx.x; i < L; i += 256) tws[i] = a.tw[i];
+    for (int i = threadIdx.x; i < L; i += NT) tws[i] = a.tw[i];
     float2* ep = fft_ct_free<L>(buf0, buf1);
     const int shift = a.h - a.pad;
     const float4* mrow = reinterpret_cast<const float4*>(a.maps + ((int64_t)row * X + x) * a.C);
@@ -828,7 +845,7 @@ __global__ void __launch_bounds__(256, (W >= 16 ? 3 : 4)) k_adj_x_tma(AdjXArgs a
             o = o >= L ? o - L : (o < 0 ? o + L : o);
             if (o < X) ep[w * XP + o] = v;
         };
-        fft_ct<L, W, 256, true>(buf0, buf1, tws, store);
+        fft_ct<L, W, NT, true>(buf0, buf1, tws, store);
         __syncthreads();                    // transform done: buf0 free (odd stage counts), ep complete
         if (kEarly && threadIdx.x == 0 && c0 + W < a.C) issue(c0 + W);
         // conj(S) product and the sum over this group's coils, in coil order
@@ -1414,7 +1431,7 @@ static tr_status launch_line(tr_plan* p, int axis, const float2* in, float2* out
     TR_TRY(set_smem_limit(fn, smem));
     if (tma) {
         void* args[] = {&la, &tin, &tout};
-        TR_CUDA(cudaLaunchKernel(fn, grid, dim3(256), args, smem, st));
+        TR_CUDA(cudaLaunchKernel(fn, grid, dim3((unsigned)ct_threads(A.L, la.W)), args, smem, st));
     } else {
         void* args[] = {&la};
         TR_CUDA(cudaLaunchKernel(fn, grid, dim3(256), args, smem, st));
@@ -1695,7 +1712,7 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
             TR_TRY(set_smem_limit(tfn, smem));
             dim3 grid((unsigned)((int64_t)Z * Y * n_img));
             void* args[] = {&aa, &tin};
-            TR_CUDA(cudaLaunchKernel(tfn, grid, dim3(256), args, smem, st));
+            TR_CUDA(cudaLaunchKernel(tfn, grid, dim3((unsigned)ct_threads(OSX, kTmaXWidth)), args, smem, st));
             return TR_OK;
         }
     }
