@@ -298,11 +298,11 @@ __host__ __device__ constexpr int ct_nstages(int L) {
     return s;
 }
 
-template <int L, int W, int NT, bool INV, int s, int Ns>
+template <int L, int W, int NT, bool INV, int s, int Ns, bool LD = false>
 struct CtStage {
-    template <class Store>
+    template <class Load, class Store>
     __device__ __forceinline__ static void run(const float2* __restrict__ src, float2* __restrict__ dst,
-                                               const float2* __restrict__ tw, Store& store) {
+                                               const float2* __restrict__ tw, Load& load, Store& store) {
         constexpr int S = ct_nstages(L);
         constexpr int R = ct_radix(L, s);
         constexpr int NB = L / R;
@@ -319,7 +319,9 @@ struct CtStage {
                 float2 v[R];
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    float2 x = src[(j + r * NB) * W + w];
+                    float2 x;
+                    if constexpr (LD && s == 0) x = load(j + r * NB, w);
+                    else x = src[(j + r * NB) * W + w];
                     if (Ns > 1 && r > 0) {
                         float2 t = tw[k * r * STEP];
                         if (INV) t.y = -t.y;
@@ -338,16 +340,28 @@ struct CtStage {
         }
         if constexpr (s < S - 1) {
             __syncthreads();
-            CtStage<L, W, NT, INV, s + 1, Ns * R>::run(dst, const_cast<float2*>(src), tw, store);
+            CtStage<L, W, NT, INV, s + 1, Ns * R, LD>::run(dst, const_cast<float2*>(src), tw, load, store);
         }
     }
 };
 
 // Transform the [L][W] tile in A (A is clobbered); the last stage hands every
 // output element to store(k, w, v).
+struct NoLoad {
+    __device__ __forceinline__ float2 operator()(int, int) const { return make_float2(0.f, 0.f); }
+};
 template <int L, int W, int NT, bool INV, class Store>
 __device__ __forceinline__ void fft_ct(float2* A, float2* B, const float2* tw, Store& store) {
-    CtStage<L, W, NT, INV, 0, 1>::run(A, B, tw, store);
+    NoLoad none;
+    CtStage<L, W, NT, INV, 0, 1>::run(A, B, tw, none, store);
+}
+
+// Same transform with the first stage reading its inputs from load(m, w)
+// (input element m of column w) instead of A: A is not read, so it may hold
+// whatever load() reads until the first stage ends.  The first stage writes B.
+template <int L, int W, int NT, bool INV, class Load, class Store>
+__device__ __forceinline__ void fft_ct_ld(float2* A, float2* B, const float2* tw, Load& load, Store& store) {
+    CtStage<L, W, NT, INV, 0, 1, true>::run(A, B, tw, load, store);
 }
 
 // Buffer that the last stage of an L-point fft_ct does not read.

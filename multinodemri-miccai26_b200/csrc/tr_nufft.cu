@@ -751,8 +751,8 @@ __global__ void __launch_bounds__(NT) k_fwd_x_tma(FwdXArgs a, const __grid_const
     float2* smB = sm + L * W;
     float2* tws = sm + 2 * L * W;
     const int X = a.X;
-    float2* s_img = smB;              // [X]
-    float2* s_map = smB + X;          // [X][W]
+    float2* s_img = smA;              // [X]     (the first FFT stage reads these and writes smB)
+    float2* s_map = smA + X;          // [X][W]
     const int img = (int)(blockIdx.x % (unsigned)a.n_img);
     const int row = (int)(blockIdx.x / (unsigned)a.n_img);
     const int c0 = (int)blockIdx.z * W;
@@ -772,20 +772,20 @@ __global__ void __launch_bounds__(NT) k_fwd_x_tma(FwdXArgs a, const __grid_const
         return;
     }
     const float apzy = s_apzy;
-#pragma unroll 4
-    for (int idx = threadIdx.x; idx < L * W; idx += NT) {
-        const int m = idx / W, w = idx - m * W;
-        int j = m + a.h;
+    const int h = a.h, pad = a.pad;
+    const float* apx = a.apx;
+    // input element m of column w: u * S * apodisation * scale at x = (m + L/2) mod L - pad, 0 outside the image
+    auto load = [=](int m, int w) {
+        int j = m + h;
         if (j >= L) j -= L;
-        const int x = j - a.pad;
+        const int x = j - pad;
         float2 v = make_float2(0.f, 0.f);
-        if (x >= 0 && x < X) v = cscale(cmul(s_img[x], s_map[x * W + w]), apzy * a.apx[x]);
-        smA[idx] = v;
-    }
-    __syncthreads();
+        if (x >= 0 && x < X) v = cscale(cmul(s_img[x], s_map[x * W + w]), apzy * apx[x]);
+        return v;
+    };
     float2* ep = fft_ct_free<L>(smA, smB);
     auto store = [ep](int k, int w, float2 v) { ep[k * W + w] = v; };
-    fft_ct<L, W, NT, false>(smA, smB, tws, store);
+    fft_ct_ld<L, W, NT, false>(smA, smB, tws, load, store);
     fence_proxy_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
