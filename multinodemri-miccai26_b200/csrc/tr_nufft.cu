@@ -1355,6 +1355,9 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 // 3-D map over complex64 data [d2][d1][d0] (8-byte elements), box [1][b1][b0].
+// Every tensor map here promotes L2 fills to 256 bytes: a 128-byte row segment
+// of a z-pass box then brings in the segment the next CTA reads (the z passes
+// measured 2 % faster than with 128-byte promotion, the other passes unchanged).
 static bool encode_map_3d(CUtensorMap* m, const void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint32_t b0,
                           uint32_t b1) {
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
@@ -1364,7 +1367,7 @@ static bool encode_map_3d(CUtensorMap* m, const void* base, uint64_t d0, uint64_
     const cuuint32_t box[3] = {b0, b1, 1};
     const cuuint32_t estr[3] = {1, 1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_INT64, 3, const_cast<void*>(base), dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -1493,7 +1496,7 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
             const cuuint32_t box[3] = {(cuuint32_t)X, 1, 1};
             const cuuint32_t estr[3] = {1, 1, 1};
             ok = enc(&timg, CU_TENSOR_MAP_DATA_TYPE_INT64, 3, const_cast<float2*>(images), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
         }
         ok = ok && encode_map_3d(&tmap, maps, (uint64_t)C, (uint64_t)X, nrows, (uint32_t)kTmaXWidth, (uint32_t)X);
@@ -1626,7 +1629,7 @@ static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, 
         const cuuint32_t box[4] = {(cuuint32_t)sa.cchunk, kTile, kTile, kSlabZ};   // one staged piece
         const cuuint32_t estr[4] = {1, 1, 1, 1};
         tma = enc && enc(&tgrid, CU_TENSOR_MAP_DATA_TYPE_INT64, 4, p->bufA, dims, strides, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
     }
     const int zper = tma ? kZeroTilesTma : kZeroTiles;

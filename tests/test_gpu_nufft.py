@@ -114,8 +114,10 @@ def test_adjoint_is_bitwise_deterministic():
                                        ((48, 64, 64), 3, 6), ((48, 64, 64), 1, 40), ((48, 64, 64), 2, 8),
                                        ((48, 64, 64), 3, 4), ((48, 64, 64), 1, 1), ((50, 64, 64), 2, 16),
                                        ((32, 48, 256), 2, 16), ((32, 48, 256), 1, 12), ((32, 48, 256), 2, 4),
-                                       ((32, 48, 256), 1, 2)])
+                                       ((32, 48, 256), 1, 2), ((51, 67, 64), 2, 24), ((51, 67, 64), 1, 8)])
 def test_batched_coil_echo_path(shape, E, C):
+    # (51, 67, 64): an odd row count (the adjoint x pass takes rows in blocks) and
+    # three 8-coil groups per row (its tile pipeline alternates two buffers)
     torch = _torch()
     nb = pkg("nufft_backend")
     rng = np.random.default_rng(E * 31 + C)
