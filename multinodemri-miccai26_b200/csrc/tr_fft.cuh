@@ -364,6 +364,69 @@ __device__ __forceinline__ void fft_ct_ld(float2* A, float2* B, const float2* tw
     CtStage<L, W, NT, INV, 0, 1, true>::run(A, B, tw, load, store);
 }
 
+// In-place variant: every stage first reads all of a thread's butterflies into
+// registers, the CTA synchronises, and the results go back into the same
+// [L][W] buffer; the last stage hands its outputs to store(k, w, v), which may
+// write into the buffer.  Same butterflies, twiddles and output order as
+// fft_ct (bit-identical results) with half the shared memory.
+template <int L, int W, int NT, bool INV, int s, int Ns>
+struct CtStageIP {
+    template <class Store>
+    __device__ __forceinline__ static void run(float2* buf, const float2* __restrict__ tw, Store& store) {
+        constexpr int S = ct_nstages(L);
+        constexpr int R = ct_radix(L, s);
+        constexpr int NB = L / R;
+        constexpr int TOTAL = NB * W;
+        constexpr int STEP = L / (Ns * R);
+        constexpr int ITERS = (TOTAL + NT - 1) / NT;
+        float2 v[ITERS][R];
+#pragma unroll
+        for (int it = 0; it < ITERS; ++it) {
+            const int idx = (int)threadIdx.x + it * NT;
+            if (TOTAL % NT == 0 || idx < TOTAL) {
+                const int j = idx / W;
+                const int w = idx - j * W;
+                const int k = (Ns == 1) ? 0 : j % Ns;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    float2 x = buf[(j + r * NB) * W + w];
+                    if (Ns > 1 && r > 0) {
+                        float2 t = tw[k * r * STEP];
+                        if (INV) t.y = -t.y;
+                        x = cmul_p(x, t);
+                    }
+                    v[it][r] = x;
+                }
+                Dft<R>::run(v[it], INV);
+            }
+        }
+        __syncthreads();                                   // every read of this stage is done
+#pragma unroll
+        for (int it = 0; it < ITERS; ++it) {
+            const int idx = (int)threadIdx.x + it * NT;
+            if (TOTAL % NT == 0 || idx < TOTAL) {
+                const int j = idx / W;
+                const int w = idx - j * W;
+                const int k = (Ns == 1) ? 0 : j % Ns;
+                const int d0 = (Ns == 1) ? j * R : (j / Ns) * Ns * R + k;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (s == S - 1) store(d0 + r * Ns, w, v[it][r]);
+                    else buf[(d0 + r * Ns) * W + w] = v[it][r];
+                }
+            }
+        }
+        if constexpr (s < S - 1) {
+            __syncthreads();
+            CtStageIP<L, W, NT, INV, s + 1, Ns * R>::run(buf, tw, store);
+        }
+    }
+};
+template <int L, int W, int NT, bool INV, class Store>
+__device__ __forceinline__ void fft_ct_ip(float2* buf, const float2* tw, Store& store) {
+    CtStageIP<L, W, NT, INV, 0, 1>::run(buf, tw, store);
+}
+
 // Buffer that the last stage of an L-point fft_ct does not read.
 template <int L>
 __device__ __forceinline__ float2* fft_ct_free(float2* A, float2* B) {

@@ -362,6 +362,17 @@ __host__ __device__ constexpr int ct_threads(int L, int W) {
     return (W <= 8 && ct_rounds(L, W, 320) < ct_rounds(L, W, 256)) ? 320 : 256;
 }
 
+// The TMA line passes transform in place (register-held butterflies, one
+// [L][W] buffer): half the shared memory, so six CTAs of 320 threads (32
+// registers each) fit on an SM; 320 threads wherever that takes fewer rounds.
+constexpr bool kLineInPlace = true;
+__host__ __device__ constexpr int line_threads(int L, int W) {
+    return ct_rounds(L, W, 320) < ct_rounds(L, W, 256) ? 320 : 256;
+}
+static size_t line_tma_smem_bytes(int L, int W) {
+    return (size_t)((kLineInPlace ? 1 : 2) * L * W + L) * sizeof(float2) + 128;
+}
+
 template <int L, int W, bool INV>
 __global__ void __launch_bounds__(256) k_line_ct(LineArgs a) {
     extern __shared__ float2 sm[];
@@ -428,16 +439,16 @@ __global__ void __launch_bounds__(256) k_line_ct(LineArgs a) {
 // Lout/2 rows leave by TMA stores (rows o = (k + h - p_out) mod L < Lout).
 // One thread issues every copy; the rest of the CTA only runs the transform.
 // The load wait is bounded: on expiry the CTA sets kDevErrTmaWait and exits.
-template <int L, int W, bool INV, int NT = ct_threads(L, W)>
-__global__ void __launch_bounds__(NT) k_line_tma(LineArgs a, const __grid_constant__ CUtensorMap tin,
+template <int L, int W, bool INV, int NT = line_threads(L, W)>
+__global__ void __launch_bounds__(NT, (NT == 320 ? 5 : 6)) k_line_tma(LineArgs a, const __grid_constant__ CUtensorMap tin,
                                                   const __grid_constant__ CUtensorMap tout) {
     extern __shared__ __align__(128) unsigned char tsm_raw[];
     __shared__ __align__(8) uint64_t bar;
     // TMA boxes start on 128-byte boundaries (the launch adds 128 bytes of slack)
     float2* tsm = reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(tsm_raw) + 127) & ~uintptr_t(127));
     float2* smA = tsm;
-    float2* smB = tsm + L * W;
-    float2* tws = tsm + 2 * L * W;
+    float2* smB = tsm + L * W;                       // second buffer (not in-place builds only)
+    float2* tws = tsm + (kLineInPlace ? 1 : 2) * L * W;
     const int q0 = (int)blockIdx.x * W;
     const int outer = (int)blockIdx.y;
     if (threadIdx.x == 0) mbar_init(&bar, 1);
@@ -453,9 +464,10 @@ __global__ void __launch_bounds__(NT) k_line_tma(LineArgs a, const __grid_consta
         if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
         return;
     }
-    float2* ep = fft_ct_free<L>(smA, smB);
+    float2* ep = kLineInPlace ? smA : fft_ct_free<L>(smA, smB);
     auto store = [ep](int k, int w, float2 v) { ep[k * W + w] = v; };
-    fft_ct<L, W, NT, INV>(smA, smB, tws, store);
+    if constexpr (kLineInPlace) fft_ct_ip<L, W, NT, INV>(smA, tws, store);
+    else fft_ct<L, W, NT, INV>(smA, smB, tws, store);
     fence_proxy_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1429,12 +1441,12 @@ static tr_status launch_line(tr_plan* p, int axis, const float2* in, float2* out
 #undef TR_LINE_CASE
     if (!fn) fn = (const void*)k_line;
     la.vec16 = ((inner % 2) == 0 && (la.W % 2) == 0 && ((uintptr_t)in % 16) == 0) ? 1 : 0;
-    const size_t smem = fft_smem_bytes(A.L, la.W) + (tma ? 128 : 0);
+    const size_t smem = tma ? line_tma_smem_bytes(A.L, la.W) : fft_smem_bytes(A.L, la.W);
     dim3 grid((unsigned)((inner + la.W - 1) / la.W), (unsigned)outer);
     TR_TRY(set_smem_limit(fn, smem));
     if (tma) {
         void* args[] = {&la, &tin, &tout};
-        TR_CUDA(cudaLaunchKernel(fn, grid, dim3((unsigned)ct_threads(A.L, la.W)), args, smem, st));
+        TR_CUDA(cudaLaunchKernel(fn, grid, dim3((unsigned)line_threads(A.L, la.W)), args, smem, st));
     } else {
         void* args[] = {&la};
         TR_CUDA(cudaLaunchKernel(fn, grid, dim3(256), args, smem, st));
