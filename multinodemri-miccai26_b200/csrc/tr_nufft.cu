@@ -346,18 +346,18 @@ __host__ __device__ constexpr int ct_width(int L) { return L >= 240 ? 8 : 16; }
 // passes keep 16-column tiles up to L = 200: 128-byte row segments).
 constexpr int kTmaXWidth = 8;
 
-// Threads per CTA of the TMA line passes and the adjoint x pass: 320 for
-// 8-column tiles whose Stockham stages then run in fewer rounds, else 256.  At
-// L = 320, W = 8 the radix-8 stages have 320 butterflies: 256 threads need two
-// rounds for them (the second a quarter full), 320 threads one; measured on the
-// 160x320x320 grid with 96 columns, the y passes gain 3-4 % and the adjoint x
-// pass 1 %.  The 16-column z passes (L = 160) and the forward x pass measured
-// slower with 320 threads and keep 256.
+// Rounds of butterflies an NT-thread CTA runs for the Stockham stages of an
+// [L][W] tile.  At L = 320, W = 8 the radix-8 stages have 320 butterflies: 256
+// threads need two rounds for them (the second a quarter full), 320 threads one.
 __host__ __device__ constexpr int ct_rounds(int L, int W, int NT) {
     int n = 0;
     for (int s = 0; s < ct_nstages(L); ++s) n += ((L / ct_radix(L, s)) * W + NT - 1) / NT;
     return n;
 }
+// Threads per CTA of the TMA adjoint x pass: 320 for 8-column tiles that then
+// take fewer rounds, else 256 (measured on the 160x320x320 grid with 96
+// columns: 1 % faster with 320; the forward x pass measured slower with 320 and
+// keeps 256).
 __host__ __device__ constexpr int ct_threads(int L, int W) {
     return (W <= 8 && ct_rounds(L, W, 320) < ct_rounds(L, W, 256)) ? 320 : 256;
 }
