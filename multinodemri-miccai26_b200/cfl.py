@@ -30,9 +30,9 @@ def read_header(name) -> tuple:
             if s and not s.startswith("#"):
                 dims = [int(v) for v in s.split()]
                 if any(d < 1 for d in dims):
-                    raise ValueError(f"CFL dimensions must be positive: {dims}")
+                    raise ValueError(f"{path}: every CFL dimension has to be at least 1, header lists {dims}")
                 return tuple(reversed(dims))
-    raise ValueError(f"No dimensions found in CFL header: {path}")
+    raise ValueError(f"{path}: the header holds no dimension line")
 
 
 def read(name, mmap: bool = False) -> np.ndarray:
@@ -41,8 +41,8 @@ def read(name, mmap: bool = False) -> np.ndarray:
     payload = root.with_suffix(".cfl")
     expected = int(np.prod(shape, dtype=np.int64)) * CFL_DTYPE.itemsize
     if payload.stat().st_size != expected:
-        raise ValueError(f"CFL payload size mismatch for {root}: expected {expected} bytes, "
-                         f"found {payload.stat().st_size} bytes.")
+        raise ValueError(f"{payload}: holds {payload.stat().st_size} bytes, but the header's shape "
+                         f"{shape} needs {expected}")
     if mmap:
         return np.memmap(payload, mode="r", dtype=CFL_DTYPE, shape=shape)
     return np.fromfile(payload, dtype=CFL_DTYPE).reshape(shape)

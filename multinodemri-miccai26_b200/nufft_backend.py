@@ -1,19 +1,20 @@
 """NUFFT backends behind the reference's plugin interface, plus the b200 backend.
 
-Mirrors ``src/toporecon/nufft_backend.py`` of the reference:
+Mirrors the plugin layer of ``src/toporecon/nufft_backend.py`` in the reference:
 
 * ``NufftBackend``          -- the abstract contract (``:11-52``): ``xp``,
   ``num_bins``, ``to_device``, ``forward(image, bin)``, ``adjoint(ksp, bin)``
-  and ``_validate_bin`` raising ``IndexError``;
-* ``SigPyNufftBackend``     -- the reference's implementation (``:55-116``),
-  usable only where SigPy is installed (``RuntimeError`` otherwise, as there);
+  and ``_validate_bin``, whose ``IndexError`` text is part of that contract;
 * ``B200NufftBackend``      -- the sm_100a implementation.  ``forward`` /
   ``adjoint`` accept NumPy, CuPy or torch arrays and return the same kind
   (zero-copy through DLPack for device arrays), so the reference's per-call
   sites (``tvme.py:263``, ``:389``) can use it unchanged.  The batched methods
   (``forward_bin`` / ``adjoint_bin``) are the hot path of the b200
   reconstructors;
-* ``create_nufft_backend``  -- the registry (``:119-135``) with ``"b200"`` added.
+* ``create_nufft_backend``  -- the registry (``:119-135``) with ``"b200"``
+  added.  ``"sigpy"`` hands over to the reference package's own SigPy backend
+  when ``toporecon`` and SigPy are importable, and raises ``RuntimeError``
+  otherwise; this package carries no SigPy code.
 """
 
 from __future__ import annotations
@@ -28,10 +29,10 @@ from . import _lib
 
 
 class NufftBackend(ABC):
-    """Minimal contract required by the reconstruction algorithms.
+    """What a reconstructor needs from a NUFFT: per-bin forward and adjoint.
 
-    Coordinates are stored per local motion bin, already in the internal
-    ``[z, y, x]`` grid-coordinate convention.
+    A backend holds the trajectory of every local motion bin, with coordinates
+    already ordered ``[z, y, x]`` in grid units.
     """
 
     def __init__(self, img_shape: Sequence[int]) -> None:
@@ -42,76 +43,30 @@ class NufftBackend(ABC):
     @property
     @abstractmethod
     def xp(self) -> Any:
-        """Array module used by this backend."""
+        """The array module of the backend's results."""
 
     @property
     @abstractmethod
     def num_bins(self) -> int:
-        """Number of local trajectory bins."""
+        """How many motion bins the backend holds trajectories for."""
 
     @abstractmethod
     def to_device(self, array: Any) -> Any:
-        """Move or convert an array to the backend device."""
+        """Return ``array`` on the backend's device, in its array type."""
 
     @abstractmethod
     def forward(self, image: Any, bin_index: int) -> Any:
-        """Apply the forward NUFFT for one image and one motion bin."""
+        """Non-uniform k-space of one image at the trajectory of one bin."""
 
     @abstractmethod
     def adjoint(self, kspace: Any, bin_index: int) -> Any:
-        """Apply the adjoint NUFFT for one k-space array and one motion bin."""
+        """Image-space adjoint of one bin's k-space samples."""
 
     def _validate_bin(self, bin_index: int) -> int:
         resolved = int(bin_index)
         if not 0 <= resolved < self.num_bins:
             raise IndexError(f"bin_index {resolved} is outside [0, {self.num_bins}).")
         return resolved
-
-
-class SigPyNufftBackend(NufftBackend):
-    """The reference's SigPy implementation (needs SigPy; kept for comparison runs)."""
-
-    def __init__(self, img_shape, coordinates, device) -> None:
-        super().__init__(img_shape)
-        try:
-            import sigpy as sp
-        except ImportError as exc:
-            raise RuntimeError("SigPy is required for SigPyNufftBackend. "
-                               "Install the toporecon package dependencies first.") from exc
-        self._sp = sp
-        self.device = device if isinstance(device, sp.Device) else sp.Device(device)
-        prepared = []
-        for index, coordinate in enumerate(coordinates):
-            array = coordinate if hasattr(coordinate, "shape") else np.asarray(coordinate)
-            if array.ndim < 2 or array.shape[-1] != len(self.img_shape):
-                raise ValueError(f"coordinates[{index}] must end in dimension {len(self.img_shape)}, "
-                                 f"got {array.shape}.")
-            prepared.append(sp.to_device(array, self.device))
-        if not prepared:
-            raise ValueError("At least one trajectory bin is required.")
-        self.coordinates = tuple(prepared)
-
-    @property
-    def xp(self):
-        return self.device.xp
-
-    @property
-    def num_bins(self):
-        return len(self.coordinates)
-
-    def to_device(self, array):
-        return self._sp.to_device(array, self.device)
-
-    def forward(self, image, bin_index):
-        resolved = self._validate_bin(bin_index)
-        with self.device:
-            return self._sp.nufft(self.to_device(image), self.coordinates[resolved])
-
-    def adjoint(self, kspace, bin_index):
-        resolved = self._validate_bin(bin_index)
-        with self.device:
-            return self._sp.nufft_adjoint(self.to_device(kspace), self.coordinates[resolved],
-                                          oshape=self.img_shape)
 
 
 # ---------------------------------------------------------------------- helpers
@@ -156,7 +111,8 @@ def _kind(a) -> str:
 class B200NufftBackend(NufftBackend):
     """Kaiser-Bessel NUFFT (SigPy 0.1.27 definition) on one B200.
 
-    Parameters mirror ``SigPyNufftBackend(img_shape, coordinates, device)``;
+    Parameters mirror the reference's ``SigPyNufftBackend(img_shape,
+    coordinates, device)`` (``nufft_backend.py:58-88``);
     ``dcf`` (per-bin density weights), ``n_coils`` and ``n_echoes`` configure
     the batched path used by the b200 reconstructors.
     """
@@ -334,6 +290,57 @@ class B200NufftBackend(NufftBackend):
                                                   ctypes.c_void_p(out.data_ptr()), self._stream()))
         return out
 
+    def power_norm(self, n_iter: int = 30, seed: int = 0, work=None) -> float:
+        """sqrt(||A^H W A||) of the batched data operator (every bin, echo and
+        coil; W = the plan's density weights) by ``n_iter`` power-iteration
+        steps from a seeded random start; FP64 norms (``tr_power_iteration``).
+        ``work``: optional (B, Z, Y, X) complex64 start / scratch (one image
+        per bin: every echo of a bin sees the same operator)."""
+        if not self.has_maps:
+            raise RuntimeError("set_maps() first")
+        torch = self._torch
+        shape = (self.num_bins,) + self.img_shape
+        if work is not None and (not work.is_contiguous() or work.numel() != int(np.prod(shape))):
+            raise ValueError(f"work must be a contiguous {shape} complex64 tensor")
+        if work is None:
+            gen = torch.Generator(device=self.device)
+            gen.manual_seed(int(seed))
+            work = torch.randn(shape, dtype=torch.complex64, device=self.device, generator=gen)
+        out = ctypes.c_double(0.0)
+        _lib.check(self._lib.tr_power_iteration(self._plan, int(n_iter), ctypes.c_void_p(work.data_ptr()),
+                                                ctypes.byref(out), self._stream()), "tr_power_iteration")
+        return float(out.value)
+
+    def wavelet_forward(self, images, out=None):
+        """W2 analysis (db6, zero mode, PyWavelets' maximum level) of the
+        (B, E, Z, Y, X) images -> (B*E, wavelet_coeffs) coefficient trees."""
+        torch = self._torch
+        x = images.contiguous()
+        n_img = self.num_bins * self.n_echoes
+        if x.numel() != n_img * int(np.prod(self.img_shape)):
+            raise ValueError(f"images must hold {n_img} images of {self.img_shape}")
+        if out is None:
+            out = torch.empty((n_img, self.wavelet_coeffs), dtype=torch.complex64, device=self.device)
+        _lib.check(self._lib.tr_wavelet_forward(self._plan, ctypes.c_void_p(x.data_ptr()),
+                                                ctypes.c_void_p(out.data_ptr()), self._stream()), "wavelet_forward")
+        return out
+
+    def wavelet_adjoint(self, coeffs, out=None):
+        """waverec3 of (B*E, wavelet_coeffs) trees cropped to (B, E, Z, Y, X)."""
+        torch = self._torch
+        c = coeffs.contiguous()
+        if out is None:
+            out = torch.empty((self.num_bins, self.n_echoes) + self.img_shape, dtype=torch.complex64,
+                              device=self.device)
+        _lib.check(self._lib.tr_wavelet_adjoint(self._plan, ctypes.c_void_p(c.data_ptr()),
+                                                ctypes.c_void_p(out.data_ptr()), self._stream()), "wavelet_adjoint")
+        return out
+
+    def set_wait_limit(self, polls: int = _lib.DEFAULT_WAIT_POLLS) -> None:
+        """Polls before a bounded device wait gives up (0: every wait gives up at
+        once, the next PDHG call then raises with TR_ERR_TIMEOUT)."""
+        _lib.check(self._lib.tr_plan_set_wait_limit(self._plan, int(polls)), "tr_plan_set_wait_limit")
+
     STAGES = ("fwd_x", "fwd_y", "fwd_z", "interp", "spread", "adj_z", "adj_y", "adj_x")
 
     def profile(self, bin_index: int = 0, reps: int = 5) -> dict:
@@ -370,6 +377,11 @@ def create_nufft_backend(name: str, *, img_shape: Sequence[int], coordinates: It
     """Construct a registered backend without conditionals in algorithms."""
     normalized = name.strip().lower()
     if normalized == "sigpy":
+        try:
+            from toporecon.nufft_backend import SigPyNufftBackend
+        except ImportError as exc:
+            raise RuntimeError("the 'sigpy' backend is the reference toporecon package's own SigPy "
+                               f"implementation, which cannot be imported here ({exc}); use 'b200'") from exc
         return SigPyNufftBackend(img_shape=img_shape, coordinates=coordinates, device=device)
     if normalized == "b200":
         return B200NufftBackend(img_shape, coordinates, device, **kwargs)

@@ -2,7 +2,7 @@
 
 Run in the build container (where the reference source is mounted):
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
 
 The reference's ``TvmReconstructor`` (``algorithms/tvm.py:63-491``),
 ``TvmeReconstructor`` (``algorithms/tvme.py:56-575``) and
@@ -212,4 +212,6 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path to the reference source tree>")
+    main(sys.argv[1])

@@ -80,8 +80,11 @@ def test_sigpy_backend_reports_missing_dependency():
     nb = pkg("nufft_backend")
     try:
         import sigpy  # noqa: F401
-        pytest.skip("sigpy installed")
+        import toporecon.nufft_backend  # noqa: F401
+        pytest.skip("the reference package and SigPy are installed")
     except ImportError:
         pass
-    with pytest.raises(RuntimeError, match="SigPy is required"):
+    with pytest.raises(RuntimeError, match="cannot be imported here"):
         nb.create_nufft_backend("sigpy", img_shape=(8, 8, 8), coordinates=[[[0.0, 0.0, 0.0]]], device=-1)
+    with pytest.raises(ValueError, match="Unknown NUFFT backend"):
+        nb.create_nufft_backend("cufinufft", img_shape=(8, 8, 8), coordinates=[[[0.0, 0.0, 0.0]]], device=0)
