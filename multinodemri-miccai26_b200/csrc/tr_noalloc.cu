@@ -1,10 +1,10 @@
 // Allocation-free variant of the PDHG stopping-tolerance reduction.
 //
 // Some callers cannot allocate device memory at the point where they need the
-// stopping test: code that enqueues work while a CUDA stream is being captured
-// into a graph (cudaMalloc is not permitted during capture), and hosts that
-// own the whole device heap themselves (a framework's pooled allocator, an
-// inference runtime's plugin enqueue) and forbid third-party allocations.
+// stopping test: hosts that own the whole device heap themselves (a
+// framework's pooled allocator, an inference runtime's plugin enqueue, an
+// embedded scanner pipeline that reserves all device memory up front) and
+// forbid a library from calling cudaMalloc / cudaFree behind their back.
 // tr_tolerance_sums_noalloc serves them: it computes the same FP64 sums as the
 // tolerance step inside tr_pdhg_run, but its per-block partial sums live in a
 // file-scope __device__ array instead of plan or cudaMalloc memory.
@@ -15,6 +15,7 @@
 // race on it and must be serialised by the caller.  Each call writes every
 // partial it later reads, so nothing has to be cleared between calls.
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -33,10 +34,29 @@ static_assert((long long)kNoallocBlocks * kNoallocThreads * kNoallocItems == TR_
 // Per-block (num, den) partial sums: 2 x 4096 doubles = 64 KiB per device.
 static __device__ __align__(256) double g_noalloc_partials[2 * kNoallocBlocks];
 
-// Device address of g_noalloc_partials, looked up once per device.
+// Device address of g_noalloc_partials, looked up once per device and
+// context: a context that is torn down and re-created (cudaDeviceReset, a host
+// that destroys its primary context) reloads the module at a new address, so
+// the cached pointer is keyed on the context current at the call.
 std::mutex g_mu;
 constexpr int kMaxDevices = 64;
 double* g_addr[kMaxDevices] = {};
+CUcontext g_ctx[kMaxDevices] = {};
+
+// cuCtxGetCurrent from the driver, looked up once (no libcuda link).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(ptr);
+    });
+    return fn;
+}
 
 __global__ void __launch_bounds__(kNoallocThreads) k_tol_partials_noalloc(const float2* __restrict__ cur,
                                                                           const float2* __restrict__ prev,
@@ -117,14 +137,22 @@ extern "C" tr_status tr_tolerance_sums_noalloc(const void* cur, const void* prev
     int dev = 0;
     TR_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return tr::fail(TR_ERR_UNSUPPORTED, "device ordinal out of range");
+    CtxGetCurrentFn get_ctx = ctx_get_current();
+    if (!get_ctx) return tr::fail(TR_ERR_CUDA, "tr_tolerance_sums_noalloc: cuCtxGetCurrent unavailable");
+    CUcontext ctx = nullptr;   // null until the runtime has made the device's context current
+    if (get_ctx(&ctx) != CUDA_SUCCESS) ctx = nullptr;
     double* scratch = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_addr[dev]) {
-            // set-up, once per device, with that device current
+        if (!ctx || !g_addr[dev] || g_ctx[dev] != ctx) {
+            // set-up, once per device (and again after its context was re-created),
+            // with that device current; the lookup also makes the primary context current
             void* ptr = nullptr;
             TR_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_partials));
+            if (get_ctx(&ctx) != CUDA_SUCCESS || !ctx)
+                return tr::fail(TR_ERR_CUDA, "tr_tolerance_sums_noalloc: no current CUDA context");
             g_addr[dev] = static_cast<double*>(ptr);
+            g_ctx[dev] = ctx;
         }
         scratch = g_addr[dev];
     }

@@ -1,9 +1,10 @@
 """The allocation-free tolerance entry point against tr_pdhg_run's own tolerance.
 
 tr_tolerance_sums_noalloc exists for callers that cannot allocate device
-memory where they run the stopping test (work enqueued during CUDA-graph
-capture, hosts that own the whole device heap).  It keeps its partial sums in
-a fixed file-scope device array instead of allocating.  Here it is called
+memory where they run the stopping test: hosts that own the whole device heap
+through their own allocator and forbid a library from calling cudaMalloc.  It
+keeps its partial sums in a fixed file-scope device array instead of
+allocating.  Here it is called
 through the C ABI on two consecutive PDHG iterates, and the tolerance it yields
 must equal the one tr_pdhg_run reported for the same iteration.  This file is
 named to be collected last, and it passes alone or after the other tests.
