@@ -10,11 +10,19 @@ available).  A "step" is one PDHG iteration over the whole batch (every bin,
 echo and coil).  W warm-up steps, then K steps timed with CUDA events on the
 solver's stream; then a full plain (zero-start) solve to tolerance and, when a
 trained network is present, a warm-started solve, each timed with CUDA events.
+Both solves use ``--step-rule`` (default ``power``: block-diagonal PDHG steps
+from the FP64 power-iteration estimate of the data operator norm, whose device
+time is part of every solve's time; ``reference``: sigma = tau = 1/6).
 
 The JSON line's ``value`` is the time-to-tolerance in seconds: the
-warm-started solve when a trained network exists and its result is within
-1e-3 relative L2 of the plain result, else the plain solve (``value_source``
-says which); inputs are resident in HBM when timing starts.
+warm-started solve when a trained network exists, it reached the tolerance and
+its result is within 1e-3 relative L2 of the plain result, else the plain
+solve (``value_source`` says which); inputs are resident in HBM when timing
+starts.  ``tol_reached_plain`` says whether the plain solve met ``--tol``
+before ``max_iter``.  ``oracle_check`` gives the relative L2 errors of the
+b200 NUFFT (against the FP64 direct NUDFT and the KB restatement) and of a
+short PDHG run with the same steps (against the FP64 PDHG oracle) on a 32^3
+crop of the workload; it runs after every timed region.
 ``e2e`` is the same solve through the public API from pinned host buffers
 (plan creation, H2D of k-space and maps, sort, solve, D2H of the image).
 ``roofline`` reports the dominant NUFFT kernel (CUDA-event time of one launch
@@ -88,6 +96,11 @@ def parse(argv=None):
                     help="time JSENSE coil-map estimation on the workload's first echo instead of PDHG")
     ap.add_argument("--sharded", action="store_true",
                     help="use the bin-sharded multi-GPU path even on one GPU (exercises its code on one device)")
+    ap.add_argument("--step-rule", choices=("power", "reference"), default="power",
+                    help="PDHG steps of the timed solves: block-diagonal steps from the FP64 power-iteration "
+                         "norm estimate (default), or the reference's sigma = tau = 1/6")
+    ap.add_argument("--no-oracle-check", action="store_true",
+                    help="skip the FP64-oracle error report on the small crop of the workload")
     return ap.parse_args(argv)
 
 
@@ -225,6 +238,54 @@ def cpu_sample(cfg, ds_coord_bins, n_pairs: int = 1):
     return per_iter, cgrid.threads(), t_pair, t_elem
 
 
+def oracle_check(cfg, step_rule: str, device: int, n_iter: int = 8) -> dict:
+    """Relative L2 errors of the b200 path against the FP64 oracle on a 32^3
+    crop of the workload (same algorithm, coupling, lambda, step rule,
+    synthetic model; 4 coils, 2 echoes, 2 bins of 128 cones x 160 readout):
+    the NUFFT against the FP64 direct NUDFT and the KB restatement, and
+    ``n_iter`` PDHG iterations against the FP64 PDHG oracle with the same steps."""
+    import torch
+    from dataclasses import replace
+    from oracle import cgrid
+    from oracle import nufft as onf
+    from oracle import pdhg as op
+    syn = importlib.import_module(f"{PKG}.synthetic")
+    solver_mod = importlib.import_module(f"{PKG}.solver")
+    nb = importlib.import_module(f"{PKG}.nufft_backend")
+    small = replace(cfg, name=cfg.name + "-crop32", img_shape=(32, 32, 32), n_coils=4,
+                    n_echoes=min(2, cfg.n_echoes), n_bins=2, n_interleaves=128, n_readout=160,
+                    binning="amplitude")
+    ds = syn.make_geometry(small)
+    syn.simulate_kspace(ds, lambda imgs, k: cgrid.nufft(imgs, k))
+    coords = [ds.coord[ds.bin_indices(b)].reshape(-1, 3) for b in range(small.n_bins)]
+    dcfs = [ds.dcf[ds.bin_indices(b)].reshape(-1) for b in range(small.n_bins)]
+    ksps = [ds.ksp[:, :, ds.bin_indices(b)].reshape(small.n_echoes, small.n_coils, -1) for b in range(small.n_bins)]
+    # NUFFT of one image at bin 0's samples: FP64 direct NUDFT and the KB restatement
+    be = nb.B200NufftBackend(small.img_shape, [coords[0]], device)
+    x = ds.truth[0, 0]
+    y = be.forward(x, 0)
+    be.close()
+    nudft = onf.nudft(x.astype(np.complex128), coords[0])
+    kb = onf.nufft(x, coords[0])
+    lam = small.lam
+    s = solver_mod.PdhgSolver(small.algorithm, small.img_shape, coords, dcfs, ds.mps, ksps, device=device,
+                              l2_coupling=small.l2_coupling, lam_m=lam, lam_e=lam, lam_w1=lam, lam_w2=lam,
+                              step_rule=step_rule, power_iters=40)
+    r = s.run(max_iter=n_iter, tol=0.0)
+    img = r.image.cpu().numpy()
+    s.close()
+    pb = op.Problem(op.OracleNufft(small.img_shape, coords), [k.astype(np.complex128) for k in ksps], dcfs, ds.mps)
+    ref = op.run(small.algorithm, pb, max_iter=n_iter, tol=0.0, sigma=r.sigma, tau=r.tau, sigma_data=r.sigma_data,
+                 lam_m=lam, lam_e=lam, lam1=lam, lam2=lam, lam3=lam, l2_coupling=small.l2_coupling)
+    torch.cuda.synchronize()
+    return {"crop": list(small.img_shape), "coils": small.n_coils, "echoes": small.n_echoes, "bins": small.n_bins,
+            "pdhg_iterations": n_iter, "step_rule": step_rule,
+            "rel_l2_pdhg_vs_fp64_pdhg": onf.rel_l2(img, ref.image),
+            "rel_l2_nufft_vs_fp64_nudft": onf.rel_l2(y, nudft),
+            "rel_l2_nufft_vs_kb_restatement": onf.rel_l2(y, kb),
+            "kb_restatement_vs_fp64_nudft": onf.rel_l2(kb, nudft)}
+
+
 def bin_coords(ds):
     return [ds.coord[ds.bin_indices(b)] for b in range(ds.cfg.n_bins)]
 
@@ -280,11 +341,15 @@ def run_b200(args):
     torch.cuda.synchronize()
     ms_step = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world, device)
 
-    # ---- plain solve to tolerance
+    # ---- plain solve to tolerance (the power rule's norm estimate is part of its time)
+    if args.step_rule == "power":
+        solver.set_power_steps()
+        log(f"power rule: ||W^1/2 A|| = {solver.data_norm:.6g} ({solver.setup_seconds:.3f}s), sigma {solver.sigma:.4g}, "
+            f"tau {solver.tau:.4g}, sigma_data {solver.sigma_data:.4g}")
     r_plain = solver.run(max_iter=cfg.max_iter, tol=cfg.tol)
     plain_img = r_plain.image.clone()
-    t_plain = max_over_ranks(r_plain.seconds, world, device)
-    log(f"plain: {r_plain.iterations} iterations, {t_plain:.3f}s")
+    t_plain = max_over_ranks(r_plain.seconds + r_plain.setup_seconds, world, device)
+    log(f"plain: {r_plain.iterations} iterations, {t_plain:.3f}s (tol {r_plain.tols[-1]:.3g})")
 
     # ---- warm-started solve (learned initial iterate), when a trained network exists
     warm = None
@@ -315,9 +380,11 @@ def run_b200(args):
                          torch.linalg.vector_norm(plain_img.reshape(-1)))
 
     # the warm-started time counts only when its answer is the plain PDHG answer
-    # (relative L2 within WARM_MATCH); otherwise the plain time is the value
-    use_warm = warm is not None and rel_warm is not None and rel_warm <= WARM_MATCH
-    value = max_over_ranks(warm.seconds if use_warm else t_plain, world, device)
+    # (relative L2 within WARM_MATCH) and it reached the tolerance; otherwise the plain time is the value
+    t_warm = None if warm is None else warm.seconds + warm.setup_seconds
+    use_warm = (warm is not None and rel_warm is not None and rel_warm <= WARM_MATCH
+                and warm.tols and warm.tols[-1] < cfg.tol)
+    value = max_over_ranks(t_warm if use_warm else t_plain, world, device)
 
     # ---- e2e through the public API from pinned host buffers
     e2e = None
@@ -335,7 +402,7 @@ def run_b200(args):
         t0 = time.perf_counter()
         s2 = solver_mod.PdhgSolver(cfg.algorithm, cfg.img_shape, coords, dcfs, mps_h, ksp_h,
                                    l2_coupling=cfg.l2_coupling, lam_m=lam, lam_e=lam, lam_w1=lam, lam_w2=lam,
-                                   use_graph=not args.no_graph, device=local)
+                                   use_graph=not args.no_graph, device=local, step_rule=args.step_rule)
         if use_warm:
             r2 = ws.warm_solve(s2, cfg, max_iter=cfg.max_iter, tol=cfg.tol)
         else:
@@ -347,6 +414,12 @@ def run_b200(args):
         e2e = {"value": round(t_e2e, 4), "unit": "s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(out_h.numel() * 8)}
         s2.close()
+
+    # ---- FP64-oracle error on a small crop of the workload (checker, outside every timed region)
+    check = None
+    if rank == 0 and world == 1 and not args.no_oracle_check:
+        check = oracle_check(cfg, args.step_rule, local)
+        log(f"oracle check: {check}")
 
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
@@ -373,15 +446,21 @@ def run_b200(args):
             "config": {"workload": cfg.name, "algorithm": cfg.algorithm, "img_shape_zyx": list(cfg.img_shape),
                        "coils": C, "echoes": E, "bins": B, "cones": cfg.n_interleaves, "readout": cfg.n_readout,
                        "tol": cfg.tol, "max_iter": cfg.max_iter, "l2_flush": "inputs larger than L2",
+                       "step_rule": args.step_rule,
                        "parallelism": "replicas" if world > 1 else "single-gpu"},
-            "value_source": "warm-started PDHG" if use_warm else "plain PDHG",
+            "value_source": ("warm-started PDHG" if use_warm else "plain PDHG") + f", {args.step_rule} step rule",
+            "steps": {"sigma": r_plain.sigma, "tau": r_plain.tau, "sigma_data": r_plain.sigma_data,
+                      "data_norm": r_plain.data_norm, "norm_estimate_s": round(r_plain.setup_seconds, 4)},
+            "tol_reached_plain": bool(r_plain.tols and r_plain.tols[-1] < cfg.tol),
             "time_to_tol_plain_s": round(t_plain, 4),
             "iterations_plain": r_plain.iterations,
             "tol_trace_plain": [round(t, 6) for t in r_plain.tols[::max(1, len(r_plain.tols) // 12)]],
-            "time_to_tol_warm_s": None if warm is None else round(warm.seconds, 4),
+            "time_to_tol_warm_s": None if warm is None else round(t_warm, 4),
             "iterations_warm": None if warm is None else warm.iterations,
-            "warm_speedup": None if warm is None else round(t_plain / warm.seconds, 3),
+            "tol_reached_warm": None if warm is None else bool(warm.tols and warm.tols[-1] < cfg.tol),
+            "warm_speedup": None if warm is None else round(t_plain / t_warm, 3),
             "rel_l2_warm_vs_plain": rel_warm,
+            "oracle_check": check,
             "iterations_per_s": round(1000.0 / ms_step, 3),
             "nufft_gbs": round(nufft_bytes / (nufft_ms * 1e6), 1),
             "nufft_stages": {k: {"ms": round(v["ms"], 4), "gbs": round(v["gbs"], 1),

@@ -86,6 +86,16 @@ tr_status tr_plan_destroy(tr_plan* plan);
 tr_status tr_plan_info(const tr_plan* plan, tr_plan_info_t* info);
 const char* tr_last_error_string(void);
 
+/* Bounded device waits.  Kernels that stage tiles by TMA wait for them on an
+ * mbarrier for at most `polls` polls (default 1 << 20); a wait that gives up
+ * lets the copies already in flight land, marks the plan's device error word
+ * and leaves its tile, and the next tr_pdhg_run / tr_pdhg_phase returns
+ * TR_ERR_TIMEOUT with the results of that iteration invalid.  polls = 0 makes
+ * every such wait give up at once, which exercises that error path without a
+ * fault.  Drops the plan's captured iteration graph.  (No counterpart in the
+ * reference, whose CuPy kernels have no device-side waits.) */
+tr_status tr_plan_set_wait_limit(tr_plan* plan, int32_t polls);
+
 /* Coil sensitivities (C, Z, Y, X) complex64 on the device; copied into the
  * plan's coil-interleaved layout.  Needed by the batched path only. */
 tr_status tr_plan_set_maps(tr_plan* plan, const void* mps, void* stream);
@@ -118,12 +128,16 @@ tr_status tr_nufft_adjoint_bin(tr_plan* plan, int32_t bin, const void* ksp_inter
 typedef struct {
     int32_t algorithm;           /* TR_ALG_* */
     int32_t l2_coupling;         /* --l2-coupling: prox over all echoes of the motion dual */
-    float sigma, tau;            /* dual / primal steps (reference: 1/6, tvme.py:968) */
+    float sigma, tau;            /* dual / primal steps (reference: 1/6, tvme.py:968); sigma is the
+                                    step of the TV and wavelet duals */
     float lam_m;                 /* motion TV (TVM lamda, TVME lamda_m, TVMW lambda1) */
     float lam_e;                 /* TVME echo-spatial TV (lamda_e) */
     float lam_w1;                /* TVMW db1 echo wavelet (lambda2) */
     float lam_w2;                /* TVMW db6 spatial wavelet (lambda3) */
     int32_t use_graph;           /* capture one iteration in a CUDA graph and replay it */
+    float sigma_data;            /* step of the data dual q; 0 means sigma (the reference's single
+                                    step, tvme.py:263-267).  A separate value gives block-diagonal
+                                    PDHG steps (no counterpart in the reference). */
 } tr_pdhg_params;
 
 /* Device state, all (B, E, Z, Y, X) complex64 unless noted; unused fields NULL.
@@ -185,12 +199,28 @@ typedef struct {
 tr_status tr_pdhg_phase(tr_plan* plan, const tr_pdhg_state* state, const tr_pdhg_params* params,
                         const tr_pdhg_shard* shard, int32_t phase, double* tol_sums, void* stream);
 
-/* Diagnostics in FP64: operator-norm estimate sqrt(||A^H W A||) of the data
- * term (A = [F_b S_c], W = density weights) by n_iter power-iteration steps
- * on caller scratch work_images (B, E, Z, Y, X), which must hold a nonzero start.
+/* Operator norm of the data term for the PDHG step rule: sqrt(||A^H W A||)
+ * (A = [F_b S_c] over every bin, echo and coil; W = density weights) by
+ * n_iter power-iteration steps.  The operator is block diagonal over (bin,
+ * echo) with the same block for every echo of a bin, so the iterate is one
+ * image per bin: caller scratch work_images (B, Z, Y, X), which must hold a
+ * nonzero start and holds the last normalised iterate on return.  Norms are
+ * reduced in FP64; the k-space scratch (total samples x C complex64) is
+ * allocated and freed inside.
  * No counterpart in the reference (it fixes sigma = tau = 1/6, tvme.py:968). */
 tr_status tr_power_iteration(tr_plan* plan, int32_t n_iter, void* work_images, double* norm_out,
                              void* stream);
+
+/* TVMW spatial wavelet W2 of every (bin, echo) image of the plan: db6, zero
+ * mode, PyWavelets' maximum level (tr_plan_info: wavelet_levels / _coeffs).
+ *   forward: coeffs (B*E, wavelet_coeffs) = wavedec3(images (B, E, Z, Y, X)),
+ *            per image [cA_L | 7 detail bands of level L | ... | level 1],
+ *            bands aad, ada, add, daa, dad, dda, ddd (letters z, y, x)
+ *   adjoint: images = waverec3(coeffs) cropped to (Z, Y, X), the operator the
+ *            reference applies in place of the adjoint.
+ * Replaces PtwtWaveletOps.w2_fwd / w2_adj (tvmw.py:196-206). */
+tr_status tr_wavelet_forward(tr_plan* plan, const void* images, void* coeffs, void* stream);
+tr_status tr_wavelet_adjoint(tr_plan* plan, const void* coeffs, void* images, void* stream);
 
 /* Per-stage device time of the batched NUFFT of one bin (all E x C columns):
  * ms[8] and the algorithmic bytes[8] of each stage, in the order
@@ -217,8 +247,8 @@ tr_status tr_conv3d_wgrad(const void* x, const void* gy, float* dw, int32_t N, i
 
 /* Allocation-free stopping-tolerance sums (no counterpart in the reference).
  * For callers that cannot allocate device memory where they run the stopping
- * test -- work enqueued while a stream is captured into a CUDA graph, or hosts
- * that own the whole device heap -- this computes in FP64 what tr_pdhg_run's
+ * test -- hosts that own the whole device heap through their own allocator and
+ * forbid cudaMalloc from a library -- this computes in FP64 what tr_pdhg_run's
  * tolerance step computes, without a plan and without allocating:
  *   TVM / TVME: sums_out = { sum |cur - prev|^2, sum |cur|^2 }
  *   TVMW:       sums_out = { sum |prev - cur|^2, sum |prev|^2 }

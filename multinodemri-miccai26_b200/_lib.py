@@ -30,8 +30,11 @@ EXPORTED = (
     "tr_plan_sort_kspace", "tr_plan_unsort_kspace", "tr_nufft_forward", "tr_nufft_adjoint",
     "tr_nufft_forward_bin", "tr_nufft_adjoint_bin", "tr_plan_bin_offset", "tr_pdhg_run",
     "tr_power_iteration", "tr_profile_nufft", "tr_tolerance_sums_noalloc", "tr_conv3d_fwd",
-    "tr_conv3d_wgrad_workspace", "tr_conv3d_wgrad", "tr_pdhg_phase",
+    "tr_conv3d_wgrad_workspace", "tr_conv3d_wgrad", "tr_pdhg_phase", "tr_plan_set_wait_limit",
+    "tr_wavelet_forward", "tr_wavelet_adjoint",
 )
+
+DEFAULT_WAIT_POLLS = 1 << 20   # bounded mbarrier waits: polls before a wait gives up
 
 
 class TrError(RuntimeError):
@@ -85,6 +88,7 @@ class PdhgParams(ctypes.Structure):
         ("lam_w1", ctypes.c_float),
         ("lam_w2", ctypes.c_float),
         ("use_graph", ctypes.c_int32),
+        ("sigma_data", ctypes.c_float),
     ]
 
 
@@ -142,6 +146,9 @@ def load() -> ctypes.CDLL:
             "tr_conv3d_wgrad": ([vp, vp, vp, i32, i32, i32, i32, i32, i32, vp, ctypes.c_size_t, vp], i32),
             "tr_pdhg_phase": ([vp, ctypes.POINTER(PdhgState), ctypes.POINTER(PdhgParams), ctypes.POINTER(PdhgShard),
                                i32, vp, vp], i32),
+            "tr_plan_set_wait_limit": ([vp, i32], i32),
+            "tr_wavelet_forward": ([vp, vp, vp, vp], i32),
+            "tr_wavelet_adjoint": ([vp, vp, vp, vp], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(lib, name)

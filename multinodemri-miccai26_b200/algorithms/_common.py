@@ -71,6 +71,9 @@ def build_parser(algorithm: str) -> argparse.ArgumentParser:
     p.add_argument("--warm-start", choices=("none", "learned"), default="none",
                    help="initial PDHG iterate: zeros (reference) or the learned network's prediction")
     p.add_argument("--no-cuda-graph", dest="cuda_graph", action="store_false")
+    p.add_argument("--step-rule", choices=("reference", "power"), default="reference",
+                   help="PDHG steps: the reference's sigma = tau = 1/6, or block-diagonal steps set by an FP64 "
+                        "power-iteration estimate of the data operator norm")
     p.add_argument("--prepared-dir", type=str, default=None)
     p.add_argument("--output-dir", type=str, default=".")
     p.add_argument("--verbose", action="store_true")
@@ -184,7 +187,7 @@ class _Reconstructor:
                  echo_right_peer=None, B_total=None, b0=None, b1=None, motion_left_peer=None,
                  motion_right_peer=None, bin_edges=None, world_comm=None, group_comm=None, leader_comm=None,
                  nccl_group=None, dist_grid=None, tagger=None, show_pbar=True, nufft_backend="b200",
-                 lam=None, warm_start=None, use_graph=True):
+                 lam=None, warm_start=None, use_graph=True, step_rule="reference"):
         if str(nufft_backend).lower() != "b200":
             raise ValueError("these reconstructors run the b200 backend; the SigPy path is the reference's own code")
         self.E = int(ksp.shape[0])
@@ -212,7 +215,8 @@ class _Reconstructor:
         self.show_pbar = show_pbar
         self.warm_start = warm_start
         self.solver = PdhgSolver(self.algorithm, self.img_shape, coords, dcfs, mps, ksps, device=device,
-                                 l2_coupling=l2_coupling, sigma=sigma, tau=tau, use_graph=use_graph, **(lam or {}))
+                                 l2_coupling=l2_coupling, sigma=sigma, tau=tau, use_graph=use_graph,
+                                 step_rule=step_rule, **(lam or {}))
         self.result = None
 
     def run(self):
@@ -305,7 +309,8 @@ def main_for(algorithm: str, argv=None) -> int:
                                     margin=0, device=args.device, E_total=prep.meta["E_total"], e0=0,
                                     e1=prep.meta["E_total"], B_total=args.num_bins, b0=0, b1=args.num_bins,
                                     bin_edges=prep.bin_edges, show_pbar=args.show_pbar, nufft_backend="b200",
-                                    warm_start=warm, use_graph=args.cuda_graph, **_lambdas(args, algorithm))
+                                    warm_start=warm, use_graph=args.cuda_graph, step_rule=args.step_rule,
+                                    **_lambdas(args, algorithm))
     image = rec.run().cpu().numpy()
     B, E = image.shape[:2]
     Z, Y, X = image.shape[-3:]
@@ -329,7 +334,8 @@ def main_for(algorithm: str, argv=None) -> int:
         "normalization": {"kspace": "global_max_magnitude", "mps": "coil_root_sum_of_squares",
                           "density": "maximum" if algorithm == "tvme" else "global_maximum_after_motion_sharding"},
         "b200": {"iterations": res.iterations, "final_tol": res.tols[-1] if res.tols else None,
-                 "pdhg_seconds": res.seconds, "sigma": res.sigma, "tau": res.tau, "warm_start": args.warm_start,
+                 "pdhg_seconds": res.seconds, "sigma": res.sigma, "tau": res.tau, "sigma_data": res.sigma_data,
+                 "step_rule": res.step_rule, "data_norm": res.data_norm, "warm_start": args.warm_start,
                  "cuda_graph": bool(args.cuda_graph), "main_seconds": time.perf_counter() - start},
     }
     with open(os.path.join(args.output_dir, "run_manifest.json"), "w", encoding="utf-8") as fh:

@@ -12,6 +12,7 @@ than the library.
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -57,14 +58,18 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     nvcc = nvcc_path()
     objdir = PKG / "_build"
     objdir.mkdir(exist_ok=True)
-    objs = []
+    cmds, objs = [], []
     for src in sources():
         obj = objdir / (src.stem + ".o")
-        cmd = [nvcc, *NVCC_FLAGS, *(extra or []), f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(src), "-o", str(obj)]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+        cmds.append([nvcc, *NVCC_FLAGS, *(extra or []), f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(src), "-o", str(obj)])
         objs.append(str(obj))
+    # one nvcc per translation unit, in parallel (the largest unit sets the build time)
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for cmd in cmds:
+            if verbose:
+                print(" ".join(cmd), flush=True)
+        for f in [ex.submit(subprocess.run, cmd, check=True) for cmd in cmds]:
+            f.result()
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", str(tmp), *objs, "-lcudart"]
     if verbose:

@@ -63,6 +63,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
+// Bounded wait for phase `parity`; when it gives up, a second bounded wait
+// (kMbarDrainLimit polls) lets the copies still in flight into this CTA's
+// shared memory land before the caller abandons the tile, so no copy completes
+// into shared memory the CTA no longer owns.  Returns the first wait's result.
+__device__ __forceinline__ bool mbar_wait_or_drain(uint64_t* bar, unsigned parity, int limit) {
+    if (mbar_wait_bounded(bar, parity, limit)) return true;
+    mbar_wait_bounded(bar, parity, kMbarDrainLimit);
+    return false;
+}
 __device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, uint64_t* bar, int x, int y, int z) {
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];\n"
@@ -372,7 +381,7 @@ __device__ __forceinline__ void fft_ct_ld(float2* A, float2* B, const float2* tw
 template <int L, int W, int NT, bool INV, int s, int Ns>
 struct CtStageIP {
     template <class Store>
-    __device__ __forceinline__ static void run(float2* buf, const float2* __restrict__ tw, Store& store) {
+    __device__ __forceinline__ static void run(float2* buf, const float2* __restrict__ tw, Store& store, int tid) {
         constexpr int S = ct_nstages(L);
         constexpr int R = ct_radix(L, s);
         constexpr int NB = L / R;
@@ -382,7 +391,7 @@ struct CtStageIP {
         float2 v[ITERS][R];
 #pragma unroll
         for (int it = 0; it < ITERS; ++it) {
-            const int idx = (int)threadIdx.x + it * NT;
+            const int idx = tid + it * NT;
             if (TOTAL % NT == 0 || idx < TOTAL) {
                 const int j = idx / W;
                 const int w = idx - j * W;
@@ -403,7 +412,7 @@ struct CtStageIP {
         __syncthreads();                                   // every read of this stage is done
 #pragma unroll
         for (int it = 0; it < ITERS; ++it) {
-            const int idx = (int)threadIdx.x + it * NT;
+            const int idx = tid + it * NT;
             if (TOTAL % NT == 0 || idx < TOTAL) {
                 const int j = idx / W;
                 const int w = idx - j * W;
@@ -418,13 +427,17 @@ struct CtStageIP {
         }
         if constexpr (s < S - 1) {
             __syncthreads();
-            CtStageIP<L, W, NT, INV, s + 1, Ns * R>::run(buf, tw, store);
+            CtStageIP<L, W, NT, INV, s + 1, Ns * R>::run(buf, tw, store, tid);
         }
     }
 };
+// tid: the calling thread's index in the CTA.  A caller that transforms several
+// tiles in a loop can pass a value the compiler cannot prove loop-invariant, so
+// the per-stage index arithmetic is recomputed per tile instead of being hoisted
+// out of the loop and held in registers across it.
 template <int L, int W, int NT, bool INV, class Store>
-__device__ __forceinline__ void fft_ct_ip(float2* buf, const float2* tw, Store& store) {
-    CtStageIP<L, W, NT, INV, 0, 1>::run(buf, tw, store);
+__device__ __forceinline__ void fft_ct_ip(float2* buf, const float2* tw, Store& store, int tid = threadIdx.x) {
+    CtStageIP<L, W, NT, INV, 0, 1>::run(buf, tw, store, tid);
 }
 
 // Buffer that the last stage of an L-point fft_ct does not read.

@@ -31,10 +31,28 @@ tr_status cuda_fail(cudaError_t err, const char* what, const char* file, int lin
         if (_s != TR_OK) return _s;                                     \
     } while (0)
 
+// Makes a plan's device current for the lifetime of the guard and restores the
+// caller's device afterwards.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 // ------------------------------------------------------------------ device error word
-// Kernels that wait on hardware (mbarrier polls) give up after kMbarPollLimit
-// polls and set a bit here; the host reads it with the tolerance scalars.
+// Kernels that wait on hardware (mbarrier polls) give up after the plan's poll
+// limit (kMbarPollLimit unless tr_plan_set_wait_limit changed it), wait at most
+// kMbarDrainLimit more polls for their own copies in flight, set a bit here and
+// leave; the host reads the word with the tolerance scalars.
 constexpr int kMbarPollLimit = 1 << 20;
+constexpr int kMbarDrainLimit = 1 << 20;
 constexpr int kDevErrTmaWait = 1;
 
 // ------------------------------------------------------------------ complex helpers
@@ -194,6 +212,7 @@ struct tr_plan {
     double* tol_dev = nullptr;   // [4]
     double* tol_host = nullptr;  // pinned [4]
     int* dev_err = nullptr;      // device error word (kDevErr* bits)
+    int poll_limit = tr::kMbarPollLimit;   // polls before a bounded mbarrier wait gives up
     int* err_host = nullptr;     // pinned copy, refreshed with the tolerance scalars
     // launch shapes
     int line_width = 16;

@@ -26,6 +26,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -113,6 +114,7 @@ struct FwdXArgs {
     float2* out;            // (Z, Y, OSX, ncol)
     int ncol;
     int* err;               // device error word (kDevErr* bits)
+    int poll;               // polls before a bounded mbarrier wait gives up
 };
 
 __global__ void __launch_bounds__(256) k_fwd_x(FwdXArgs a) {
@@ -176,6 +178,7 @@ struct LineArgs {
     const float2* tw;
     FftStages S;
     int* err;               // device error word (kDevErr* bits)
+    int poll;               // polls before a bounded mbarrier wait gives up
     int kA, kB;             // TMA variant: first transform row of each output box
 };
 
@@ -261,6 +264,7 @@ struct AdjXArgs {
     int64_t img_stride;
     int accumulate;
     int* err;               // device error word (kDevErr* bits)
+    int poll;               // polls before a bounded mbarrier wait gives up
 };
 
 __global__ void __launch_bounds__(256) k_adj_x(AdjXArgs a) {
@@ -436,7 +440,8 @@ __global__ void __launch_bounds__(256) k_line_ct(LineArgs a) {
 // transform runs in place in that tile (fft_ct_ip), and two boxes of
 // Lout/2 rows leave by TMA stores (rows o = (k + h - p_out) mod L < Lout).
 // One thread issues every copy; the rest of the CTA only runs the transform.
-// The load wait is bounded: on expiry the CTA sets kDevErrTmaWait and exits.
+// The load wait is bounded: on expiry the CTA waits (bounded) for its copies
+// in flight, sets kDevErrTmaWait and exits.
 template <int L, int W, bool INV, int NT = line_threads(L, W)>
 __global__ void __launch_bounds__(NT, (NT == 320 ? 5 : 6))
     k_line_tma(LineArgs a, const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout) {
@@ -456,7 +461,7 @@ __global__ void __launch_bounds__(NT, (NT == 320 ? 5 : 6))
         tma_load_3d(smA + (L / 2) * W, &tin, &bar, q0, -a.p_in, outer);
     }
     for (int i = threadIdx.x; i < L; i += NT) tws[i] = a.tw[i];
-    const bool ok = mbar_wait_bounded(&bar, 0, kMbarPollLimit);
+    const bool ok = mbar_wait_or_drain(&bar, 0, a.poll);
     if (__syncthreads_or(!ok)) {          // every thread leaves together
         if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
         return;
@@ -774,7 +779,7 @@ __global__ void __launch_bounds__(NT) k_fwd_x_tma(FwdXArgs a, const __grid_const
         s_apzy = a.apz[z] * a.apy[y] * a.scale;
     }
     for (int i = threadIdx.x; i < L; i += NT) tws[i] = a.tw[i];
-    const bool ok = mbar_wait_bounded(&bar, 0, kMbarPollLimit);
+    const bool ok = mbar_wait_or_drain(&bar, 0, a.poll);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
         return;
@@ -843,7 +848,7 @@ __global__ void __launch_bounds__(NT, (W >= 16 || NT > 256 ? 3 : 4)) k_adj_x_tma
 #pragma unroll
             for (int q = 0; q < W / 2; ++q) m2[q] = mrow[(c0 >> 1) + q];
         }
-        const bool ok = mbar_wait_bounded(&bar, (unsigned)phase, kMbarPollLimit);
+        const bool ok = mbar_wait_or_drain(&bar, (unsigned)phase, a.poll);
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
             return;
@@ -876,6 +881,100 @@ __global__ void __launch_bounds__(NT, (W >= 16 || NT > 256 ? 3 : 4)) k_adj_x_tma
         if (a.accumulate) v = cadd(*dst, v);
         *dst = v;
     }
+}
+
+// In-place adjoint x pass: two [L][W] tiles, so the first two coil groups'
+// loads are in flight together and group g + 2 loads into the tile group g
+// has finished with; each tile is transformed in place (fft_ct_ip) and its
+// last stage writes the cropped rows over the same tile in [W][XP] order; the
+// coil maps are read from global memory (L2: the n_img CTAs of a row share
+// them) in the epilogue instead of being held in registers across the
+// transform.  Same butterflies, crop, coil order and sums as k_adj_x_tma (the
+// same bits), fewer registers, so five CTAs of 320 threads share an SM.
+template <int L, int W, int MINB, int NT = ct_threads(L, W)>
+__global__ void __launch_bounds__(NT, MINB) k_adj_x_tma2(AdjXArgs a, const __grid_constant__ CUtensorMap tin) {
+    extern __shared__ __align__(128) unsigned char xsm_raw[];
+    __shared__ __align__(8) uint64_t bar[2];
+    float2* sm = align128(xsm_raw);
+    float2* tws = sm + 2 * L * W;
+    const int X = a.X;                      // <= NT: thread x owns image column x
+    const int XP = X + 4;                   // padded row of the [W][XP] epilogue (X + 4 <= L)
+    const int img = (int)(blockIdx.x % (unsigned)a.n_img);
+    const int row = (int)(blockIdx.x / (unsigned)a.n_img);
+    const int x = threadIdx.x;
+    const int ngroups = a.C / W;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+    }
+    for (int i = threadIdx.x; i < L; i += NT) tws[i] = a.tw[i];
+    __syncthreads();                        // barriers initialised
+    auto issue = [&](int g) {
+        float2* t = sm + (g & 1) * (L * W);
+        uint64_t* b = &bar[g & 1];
+        mbar_expect_tx(b, (unsigned)(L * W * sizeof(float2)));
+        const int col = img * a.C + g * W;
+        tma_load_3d(t, &tin, b, col, L / 2, row);
+        tma_load_3d(t + (L / 2) * W, &tin, b, col, 0, row);
+    };
+    if (threadIdx.x == 0) {
+        issue(0);
+        if (ngroups > 1) issue(1);
+    }
+    const int shift = a.h - a.pad;
+    const float4* mrow = reinterpret_cast<const float4*>(a.maps + ((int64_t)row * X + x) * a.C);
+    float2 s = make_float2(0.f, 0.f);
+#pragma unroll 1
+    for (int g = 0; g < ngroups; ++g) {
+        float2* t = sm + (g & 1) * (L * W);
+        const bool ok = mbar_wait_or_drain(&bar[g & 1], (unsigned)((g >> 1) & 1), a.poll);
+        if (__syncthreads_or(!ok)) {
+            // the other tile's copy (group g + 1) is in flight too: let it land before leaving
+            if (g + 1 < ngroups) mbar_wait_bounded(&bar[(g + 1) & 1], (unsigned)(((g + 1) >> 1) & 1), kMbarDrainLimit);
+            if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
+            return;
+        }
+        float2* ep = t;
+        auto store = [ep, shift, X, XP](int k, int w, float2 v) {
+            int o = k + shift;
+            o = o >= L ? o - L : (o < 0 ? o + L : o);
+            if (o < X) ep[w * XP + o] = v;
+        };
+        int tid;                            // threadIdx.x, opaque to loop-invariant code motion
+        asm volatile("mov.u32 %0, %%tid.x;" : "=r"(tid));
+        fft_ct_ip<L, W, NT, true>(t, tws, store, tid);
+        __syncthreads();                    // ep complete
+        if (x < X) {
+#pragma unroll
+            for (int q = 0; q < W / 2; ++q) {
+                const float4 m = mrow[((g * W) >> 1) + q];
+                s = cadd(s, cmulc(ep[(2 * q) * XP + x], make_float2(m.x, m.y)));
+                s = cadd(s, cmulc(ep[(2 * q + 1) * XP + x], make_float2(m.z, m.w)));
+            }
+        }
+        if (g + 2 < ngroups) {
+            fence_proxy_async_smem();       // this tile's generic-proxy accesses before the next TMA write
+            __syncthreads();                // every read of ep is done: the tile is free
+            if (threadIdx.x == 0) issue(g + 2);
+        }
+    }
+    if (x < X) {
+        const int z = row / a.Y, y = row - z * a.Y;
+        float2 v = cscale(s, a.apz[z] * a.apy[y] * a.scale * a.apx[x]);
+        float2* dst = a.img + (int64_t)img * a.img_stride + (int64_t)row * X + x;
+        if (a.accumulate) v = cadd(*dst, v);
+        *dst = v;
+    }
+}
+
+// Kernel variants selected by TOPORECON_B200_KERNELS (comparison runs of the
+// variants kept during tuning); empty: the defaults.
+static bool kernel_variant(const char* name) {
+    static const std::string sel = [] {
+        const char* e = std::getenv("TOPORECON_B200_KERNELS");
+        return std::string(e ? e : "");
+    }();
+    return sel.find(name) != std::string::npos;
 }
 
 // ------------------------------------------------------------------ per-sample tap records
@@ -1025,6 +1124,7 @@ struct SpreadArgs {
     int n_busy, n_empty, n_work;
     float2* partials;          // [slot][64 points][ncol] partial tiles of split lists
     int* err;                  // device error word (kDevErr* bits)
+    int poll;                  // polls before a bounded mbarrier wait gives up
     const float2* vals;        // (M_b, ncol) bin base
     int ncol, cchunk;          // columns per CTA (blockIdx.y selects the chunk)
     int use_dcf;
@@ -1180,7 +1280,7 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : (CG >= 4 ? 4 : 5))) k_spre
             }
         }
         if constexpr (TMA) {
-            const bool ok = mbar_wait_bounded(&bar, phase, kMbarPollLimit);
+            const bool ok = mbar_wait_or_drain(&bar, phase, a.poll);
             if (__syncthreads_or(!ok)) {
                 if (tid == 0) atomicOr(a.err, kDevErrTmaWait);
                 return;
@@ -1420,6 +1520,7 @@ static tr_status launch_line(tr_plan* p, int axis, const float2* in, float2* out
     la.tw = A.twiddle;
     la.S = stages_of(A);
     la.err = p->dev_err;
+    la.poll = p->poll_limit;
     la.kA = la.kB = 0;
     const void* fn = nullptr;
     CUtensorMap tin, tout;
@@ -1491,6 +1592,7 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
     fa.out = p->bufA;
     fa.ncol = n_img * C;
     fa.err = p->dev_err;
+    fa.poll = p->poll_limit;
     // TMA variant: one image row x kTmaXWidth coils per CTA
     if (p->use_tma && ct && maps && C % kTmaXWidth == 0 && X % 16 == 0 && X <= 256 && img_stride % 2 == 0 &&
         (int64_t)X * (kTmaXWidth + 1) <= (int64_t)OSX * kTmaXWidth && OSX / 2 <= 256) {
@@ -1624,6 +1726,7 @@ static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, 
     sa.nt1 = p->ntile[1];
     sa.nt2 = p->ntile[2];
     sa.err = p->dev_err;
+    sa.poll = p->poll_limit;
     const int cg = (sa.cchunk + 15) / 16;
     // TMA path: even column counts and chunks, 16-byte aligned k-space rows, an encodable grid map
     CUtensorMap tgrid;
@@ -1710,11 +1813,13 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
     aa.img_stride = img_stride;
     aa.accumulate = 0;
     aa.err = p->dev_err;
+    aa.poll = p->poll_limit;
     // TMA variant: one image row per CTA, coil groups of kTmaXWidth
     if (p->use_tma && ct && maps && C % kTmaXWidth == 0 && OSX / 2 <= 256 && X <= 256 && X + 4 <= OSX) {
         CUtensorMap tin;
         const void* tfn = nullptr;
-#define TR_ADJX_TMA(LV) case LV: tfn = (const void*)k_adj_x_tma<LV, kTmaXWidth>; break;
+        const int v2 = kernel_variant("adjx2") ? 4 : kernel_variant("adjx3") ? 5 : 0;
+#define TR_ADJX_TMA(LV) case LV: tfn = v2 == 4 ? (const void*)k_adj_x_tma2<LV, kTmaXWidth, 4> : v2 == 5 ? (const void*)k_adj_x_tma2<LV, kTmaXWidth, 5> : (const void*)k_adj_x_tma<LV, kTmaXWidth>; break;
         switch (OSX) { TR_CT_LENGTHS(TR_ADJX_TMA) default: break; }
 #undef TR_ADJX_TMA
         if (tfn && encode_map_3d(&tin, p->bufA, (uint64_t)aa.ncol, (uint64_t)OSX, (uint64_t)Z * Y, (uint32_t)kTmaXWidth,
@@ -1926,17 +2031,6 @@ static void plan_free(tr_plan* p) {
     cudaSetDevice(cur);
     delete p;
 }
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        if (prev >= 0) cudaSetDevice(prev);
-    }
-};
 
 // Tiles of one axis met by the KB support of coordinate k: the first tap
 // ceil(k - 2) (in double, as the device's axis_taps), four taps, and a fifth
@@ -2292,6 +2386,14 @@ tr_status tr_plan_info(const tr_plan* p, tr_plan_info_t* info) {
     info->wavelet_levels = 0;
     info->wavelet_coeffs = 0;
     wavelet_info(p, &info->wavelet_levels, &info->wavelet_coeffs);
+    return TR_OK;
+}
+
+tr_status tr_plan_set_wait_limit(tr_plan* p, int32_t polls) {
+    if (!p) return fail(TR_ERR_INVALID_ARG, "tr_plan_set_wait_limit: null plan");
+    if (polls < 0) return fail(TR_ERR_INVALID_ARG, "tr_plan_set_wait_limit: polls must be >= 0");
+    p->poll_limit = polls;
+    pdhg_destroy(p);   // a captured iteration holds the old limit in its kernel parameters
     return TR_OK;
 }
 

@@ -312,6 +312,7 @@ static tr_status validate(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_para
         return fail(TR_ERR_INVALID_ARG, "TVMW needs p_w1, p_w2, w2adj");
     if (q->algorithm < 0 || q->algorithm > 2) return fail(TR_ERR_INVALID_ARG, "unknown algorithm");
     if (!(q->sigma > 0.f) || !(q->tau > 0.f)) return fail(TR_ERR_INVALID_ARG, "sigma and tau must be positive");
+    if (!(q->sigma_data >= 0.f)) return fail(TR_ERR_INVALID_ARG, "sigma_data must be >= 0 (0: use sigma)");
     return TR_OK;
 }
 
@@ -370,10 +371,11 @@ static tr_status enqueue_phase1(tr_plan* p, const tr_pdhg_state* s, const tr_pdh
     // TVMW: the spatial-wavelet dual reads u_bar before anything changes it
     if (q->algorithm == TR_ALG_TVMW)
         TR_TRY(wavelet_dual(p, ubar, (float2*)s->p_w2, q->sigma, q->lam_w2, st));
-    // 1. data dual
+    // 1. data dual (its own step when the caller gives one)
+    const float sigma_data = q->sigma_data > 0.f ? q->sigma_data : q->sigma;
     for (int b = 0; b < p->B; ++b) {
         const int64_t off = p->bins[b].offset * ncol;
-        TR_TRY(nufft_forward_cols(p, b, ubar + (int64_t)b * EN, N, p->E, p->maps, p->C, kInterpDualProx, q->sigma,
+        TR_TRY(nufft_forward_cols(p, b, ubar + (int64_t)b * EN, N, p->E, p->maps, p->C, kInterpDualProx, sigma_data,
                                   y + off, qd + off, st));
     }
     // 2. TV / W1 duals
@@ -579,51 +581,90 @@ __global__ void k_scale(float2* x, int64_t n, const double* nrm2) {
     x[i] = make_float2((float)(x[i].x * inv), (float)(x[i].y * inv));
 }
 
-// Power iteration on A^H W A with A = [F_b S_c] over all bins and echoes and W
-// the density weights (the operator the PDHG data term sees).  work_images is
-// caller scratch of (B, E, Z, Y, X) complex64; a k-space scratch is allocated.
-extern "C" tr_status tr_power_iteration(tr_plan* p, int32_t n_iter, void* work_images, double* norm_out,
-                                        void* stream) {
-    if (!p || !work_images || !norm_out || n_iter < 1) return fail(TR_ERR_INVALID_ARG, "tr_power_iteration: bad argument");
-    if (!p->maps) return fail(TR_ERR_INVALID_ARG, "coil maps not set (tr_plan_set_maps)");
-    cudaStream_t st = (cudaStream_t)stream;
+// Device scratch owned by one call, freed on every return path.
+struct DevBuf {
+    void* ptr = nullptr;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() {
+        if (ptr) cudaFree(ptr);
+    }
+};
+
+// ||x||^2 in FP64 into d2[0] (fixed-order: block partials, then one block).
+static tr_status norm2_async(const float2* x, int64_t n, double* part, int nb, double* d2, cudaStream_t st) {
+    k_norm2<<<nb, 256, 0, st>>>(x, n, part);
+    TR_CHECK_LAUNCH();
+    k_tol_finalize<<<1, 256, 0, st>>>(part, nb, d2);
+    TR_CHECK_LAUNCH();
+    return TR_OK;
+}
+
+// Power iteration on A^H W A with A = [F_b S_c] and W the density weights (the
+// operator the PDHG data term sees; the reference has no such estimate).  The
+// operator is block diagonal over (bin, echo) and every echo of a bin sees the
+// same block, so one image per bin carries the whole spectrum: x is (B, Z, Y, X).
+// Each step normalises x, applies the forward and density-weighted adjoint
+// NUFFT over the C coil columns of every bin, and reads ||A^H W A x|| (FP64),
+// which tends to the largest eigenvalue lambda; the norm returned is
+// sqrt(lambda).
+static tr_status power_impl(tr_plan* p, int n_iter, float2* x, double* norm_out, cudaStream_t st) {
     const int64_t N = (int64_t)p->n[0] * p->n[1] * p->n[2];
-    const int64_t EN = (int64_t)p->E * N;
+    const int64_t EN = N;                 // one image per bin
     const int64_t tot = (int64_t)p->B * EN;
-    const int ncol = p->E * p->C;
-    float2* x = (float2*)work_images;
-    float2* ksp = nullptr;
-    double* part = nullptr;
-    double* d2 = nullptr;
-    TR_CUDA(cudaMalloc(&ksp, (size_t)std::max<int64_t>(p->total, 1) * ncol * sizeof(float2)));
+    const int ncol = p->C;
     const int nb = 1024;
-    TR_CUDA(cudaMalloc(&part, 2 * nb * sizeof(double)));
-    TR_CUDA(cudaMalloc(&d2, 2 * sizeof(double)));
-    tr_status rs = TR_OK;
+    DevBuf ksp, part, d2;
+    TR_CUDA(cudaMalloc(&ksp.ptr, (size_t)std::max<int64_t>(p->total, 1) * ncol * sizeof(float2)));
+    TR_CUDA(cudaMalloc(&part.ptr, 2 * nb * sizeof(double)));
+    TR_CUDA(cudaMalloc(&d2.ptr, 2 * sizeof(double)));
+    float2* kd = (float2*)ksp.ptr;
+    double* pd = (double*)part.ptr;
+    double* dd = (double*)d2.ptr;
+    double h[2] = {0.0, 0.0};
+    TR_TRY(norm2_async(x, tot, pd, nb, dd, st));
+    TR_CUDA(cudaMemcpyAsync(h, dd, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    TR_CUDA(cudaStreamSynchronize(st));
+    if (!(h[0] > 0.0) || !std::isfinite(h[0]))
+        return fail(TR_ERR_INVALID_ARG, "tr_power_iteration: the start vector is zero or not finite");
     double lam = 0.0;
-    for (int it = 0; it < n_iter && rs == TR_OK; ++it) {
-        k_norm2<<<nb, 256, 0, st>>>(x, tot, part);
-        k_tol_finalize<<<1, 256, 0, st>>>(part, nb, d2);
-        k_scale<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(x, tot, d2);
-        for (int b = 0; b < p->B && rs == TR_OK; ++b)
-            rs = nufft_forward_cols(p, b, x + b * EN, N, p->E, p->maps, p->C, kInterpStore, 0.f, nullptr,
-                                    ksp + p->bins[b].offset * ncol, st);
-        for (int b = 0; b < p->B && rs == TR_OK; ++b)
-            rs = nufft_adjoint_cols(p, b, ksp + p->bins[b].offset * ncol, p->E, p->maps, p->C, true, x + b * EN, N, st);
-        if (rs != TR_OK) break;
-        k_norm2<<<nb, 256, 0, st>>>(x, tot, part);
-        k_tol_finalize<<<1, 256, 0, st>>>(part, nb, d2);
-        double h[2];
-        cudaMemcpyAsync(h, d2, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
-        if (cudaStreamSynchronize(st) != cudaSuccess) {
-            rs = fail(TR_ERR_CUDA, "power iteration failed");
-            break;
+    for (int it = 0; it < n_iter; ++it) {
+        k_scale<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(x, tot, dd);   // x <- x / ||x||
+        TR_CHECK_LAUNCH();
+        for (int b = 0; b < p->B; ++b)
+            TR_TRY(nufft_forward_cols(p, b, x + b * EN, N, 1, p->maps, p->C, kInterpStore, 0.f, nullptr,
+                                      kd + p->bins[b].offset * ncol, st));
+        for (int b = 0; b < p->B; ++b)
+            TR_TRY(nufft_adjoint_cols(p, b, kd + p->bins[b].offset * ncol, 1, p->maps, p->C, true, x + b * EN, N,
+                                      st));
+        TR_TRY(norm2_async(x, tot, pd, nb, dd, st));
+        TR_CUDA(cudaMemcpyAsync(h, dd, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        TR_CUDA(cudaMemcpyAsync(p->err_host, p->dev_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        TR_CUDA(cudaStreamSynchronize(st));
+        if (*p->err_host != 0) {
+            *p->err_host = 0;
+            TR_CUDA(cudaMemsetAsync(p->dev_err, 0, sizeof(int), st));
+            return fail(TR_ERR_TIMEOUT, "tr_power_iteration: a bounded device wait expired in step " +
+                                            std::to_string(it));
         }
+        if (!std::isfinite(h[0]))
+            return fail(TR_ERR_NONFINITE, "tr_power_iteration: non-finite norm in step " + std::to_string(it));
         lam = std::sqrt(h[0]);  // ||A^H W A x|| with ||x|| = 1
     }
-    cudaFree(ksp);
-    cudaFree(part);
-    cudaFree(d2);
-    if (rs == TR_OK) *norm_out = std::sqrt(lam);
-    return rs;
+    // leave the normalised last iterate in x
+    k_scale<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(x, tot, dd);
+    TR_CHECK_LAUNCH();
+    TR_CUDA(cudaStreamSynchronize(st));
+    *norm_out = std::sqrt(lam);
+    return TR_OK;
+}
+
+extern "C" tr_status tr_power_iteration(tr_plan* p, int32_t n_iter, void* work_images, double* norm_out,
+                                        void* stream) {
+    if (!p || !work_images || !norm_out || n_iter < 1)
+        return fail(TR_ERR_INVALID_ARG, "tr_power_iteration: bad argument");
+    if (!p->maps) return fail(TR_ERR_INVALID_ARG, "coil maps not set (tr_plan_set_maps)");
+    DeviceGuard g(p->device);
+    return power_impl(p, n_iter, (float2*)work_images, norm_out, (cudaStream_t)stream);
 }

@@ -16,6 +16,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cfloat>
 #include <cmath>
 #include <vector>
 
@@ -403,3 +404,27 @@ tr_status wavelet_adjoint(tr_plan* p, const float2* p_w2, float2* out, cudaStrea
 }
 
 }  // namespace tr
+
+using namespace tr;
+
+// W2 analysis alone: the dual update of wavelet_dual with a zero dual, unit step
+// and an inactive projection (p = 0 + 1 c, scale min(1, FLT_MAX / |c|) = 1) is
+// the coefficient tree itself, bit for bit.
+extern "C" tr_status tr_wavelet_forward(tr_plan* p, const void* images, void* coeffs, void* stream) {
+    if (!p || !images || !coeffs) return fail(TR_ERR_INVALID_ARG, "tr_wavelet_forward: null argument");
+    if (!p->wav || p->wav->levels == 0)
+        return fail(TR_ERR_UNSUPPORTED, "image too small for a db6 decomposition");
+    DeviceGuard g(p->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t bytes = (size_t)p->B * p->E * p->wav->ncoef * sizeof(float2);
+    TR_CUDA(cudaMemsetAsync(coeffs, 0, bytes, st));
+    return wavelet_dual(p, (const float2*)images, (float2*)coeffs, 1.0f, FLT_MAX, st);
+}
+
+extern "C" tr_status tr_wavelet_adjoint(tr_plan* p, const void* coeffs, void* images, void* stream) {
+    if (!p || !images || !coeffs) return fail(TR_ERR_INVALID_ARG, "tr_wavelet_adjoint: null argument");
+    if (!p->wav || p->wav->levels == 0)
+        return fail(TR_ERR_UNSUPPORTED, "image too small for a db6 decomposition");
+    DeviceGuard g(p->device);
+    return wavelet_adjoint(p, (const float2*)coeffs, (float2*)images, (cudaStream_t)stream);
+}

@@ -5,12 +5,21 @@ The state the reference keeps as CuPy arrays (``pdhg_init``, ``tvme.py:190-205``
 device, and every iteration runs inside ``tr_pdhg_run`` (one CUDA graph per
 iteration after the first).  ``run`` reproduces ``*Reconstructor.run``:
 the stopping rule, the returned extrapolated image ``u_bar``, and the
-``OverflowError`` retry that shrinks sigma and tau by 0.9 (``tvme.py:571-573``).
+``OverflowError`` retry that shrinks the steps by 0.9 (``tvme.py:571-573``).
+
+Step rules.  ``"reference"`` keeps the reference's sigma = tau = 1/6 for every
+dual (``tvme.py:968``, ``tvm.py:991-992``, ``tvmw.py:1154``): the parity mode.
+``"power"`` sets block-diagonal steps from operator norms (``power_steps``):
+the data operator's norm ||W^1/2 A|| by an FP64 power iteration on the
+device (``tr_power_iteration``) and known bounds of the regulariser operators.
+Both rules have the same fixed points (the saddle point of the same
+objective); only the path to them differs.
 """
 
 from __future__ import annotations
 
 import ctypes
+import math
 import time
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
@@ -21,6 +30,49 @@ from . import _lib
 from .nufft_backend import B200NufftBackend
 
 
+STEP_RULES = ("reference", "power")
+
+# Squared norm bounds of the stacked regulariser operator of each algorithm.  A
+# forward difference with a zero last row has ||D||^2 <= 4, so: TVM the motion
+# difference (4); TVME the motion difference plus the echo difference followed
+# by the 3-D spatial gradient (4 + 4 * 12); TVMW the motion difference, the db1
+# echo transform and the db6 spatial analysis (both norm <= 1; 2 is kept for
+# the db6 tree as a margin).
+REG_NORM2 = {"tvm": 4.0, "tvme": 52.0, "tvmw": 7.0}
+
+
+# The power iteration approaches ||W^1/2 A|| from below (20 steps measured 0.4 %
+# low on the 256 x 256 x 128 cones workload); the step rule uses the estimate
+# times this margin.
+NORM_MARGIN = 1.02
+
+
+def power_steps(algorithm: str, data_norm: float, sigma_data: float = 0.1, data_share: float = 0.9):
+    """Block-diagonal PDHG steps (sigma, tau, sigma_data) from the data norm.
+
+    PDHG with a dual step per block (Pock & Chambolle, ICCV 2011) converges
+    when tau * (sigma_data ||W^1/2 A||^2 + sigma ||K_reg||^2) < 1.  The data
+    block takes ``data_share`` of that budget with a small dual step
+    ``sigma_data`` (the per-mode rate of the quadratic data term is best for
+    sigma_data in 0.1-0.5 with tau * sigma_data * ||A||^2 close to 1; on the
+    128 x 128 x 96 TVME workload 0.1 gave the smallest tolerance and the
+    result closest to a 1,500-iteration solve after 300 iterations), the
+    regulariser duals the rest, 1 % short of the bound.  The reference's
+    sigma = tau = 1/6 gives tau * sigma_data * ||A||^2 = ||A||^2 / 36, far
+    below 1 when ||A||^2 is small.
+    """
+    alg = algorithm.lower()
+    if alg not in REG_NORM2:
+        raise ValueError(f"unknown algorithm {algorithm!r}")
+    if not (data_norm > 0.0 and math.isfinite(data_norm)):
+        raise ValueError(f"the data operator norm must be positive and finite, got {data_norm}")
+    if not (0.0 < data_share < 1.0) or not sigma_data > 0.0:
+        raise ValueError("need 0 < data_share < 1 and sigma_data > 0")
+    tau = data_share / (sigma_data * data_norm * data_norm)
+    sigma = (1.0 - data_share) * 0.99 / (tau * REG_NORM2[alg])
+    return sigma, tau, sigma_data
+
+
 @dataclass
 class SolveResult:
     image: object                 # torch complex64 (B, E, Z, Y, X): u_bar
@@ -29,6 +81,10 @@ class SolveResult:
     seconds: float = 0.0          # device time of the PDHG iterations (CUDA events)
     sigma: float = 1 / 6
     tau: float = 1 / 6
+    sigma_data: float = 1 / 6
+    step_rule: str = "reference"
+    data_norm: Optional[float] = None     # ||W^1/2 A|| of the power rule
+    setup_seconds: float = 0.0            # device time of the norm estimate (power rule)
 
 
 class PdhgSolver:
@@ -41,7 +97,8 @@ class PdhgSolver:
     def __init__(self, algorithm: str, img_shape: Sequence[int], coords, dcf, mps, ksp, *, device=0,
                  l2_coupling: bool = False, sigma: float = 1 / 6, tau: float = 1 / 6, lam_m: float = 1e-5,
                  lam_e: float = 1e-5, lam_w1: float = 1e-5, lam_w2: float = 1e-5, use_graph: bool = True,
-                 backend: Optional[B200NufftBackend] = None, autotune: bool = True):
+                 backend: Optional[B200NufftBackend] = None, autotune: bool = True, step_rule: str = "reference",
+                 power_iters: int = 20):
         import torch
         self.torch = torch
         self.algorithm = algorithm.lower()
@@ -58,7 +115,14 @@ class PdhgSolver:
         self.device = self.backend.device
         self.stream = torch.cuda.Stream(self.device)
         self.l2_coupling = bool(l2_coupling)
+        if step_rule not in STEP_RULES:
+            raise ValueError(f"step_rule must be one of {STEP_RULES}, got {step_rule!r}")
+        self.step_rule = step_rule
+        self.power_iters = int(power_iters)
         self.sigma, self.tau = float(sigma), float(tau)
+        self.sigma_data = self.sigma
+        self.data_norm = None
+        self.setup_seconds = 0.0
         self.lam = dict(lam_m=float(lam_m), lam_e=float(lam_e), lam_w1=float(lam_w1), lam_w2=float(lam_w2))
         self.use_graph = bool(use_graph)
         ncol = self.E * self.C
@@ -73,6 +137,31 @@ class PdhgSolver:
                 self.backend.sort_kspace(kb, b, out=self.y[off:off + cnt])
         self.stream.synchronize()
         self._alloc_state()
+        if self.step_rule == "power":
+            self.set_power_steps()
+
+    def set_power_steps(self, n_iter: Optional[int] = None, sigma_data: float = 0.1, data_share: float = 0.9):
+        """Estimate ||W^1/2 A|| on the device (FP64 power iteration on one image
+        per bin, in the first B images of the state ``g`` as scratch) and set
+        the block-diagonal steps of ``power_steps`` from the estimate times
+        ``NORM_MARGIN``; the device time goes to ``setup_seconds``."""
+        torch = self.torch
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        gen = torch.Generator(device=self.device)
+        gen.manual_seed(0)
+        shape = (self.B,) + self.img_shape
+        with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+            start.record(self.stream)
+            work = self.g.view(-1)[: self.B * int(np.prod(self.img_shape))].view(shape)
+            work.copy_(torch.randn(shape, dtype=torch.complex64, device=self.device, generator=gen))
+            self.data_norm = self.backend.power_norm(self.power_iters if n_iter is None else int(n_iter), work=work)
+            stop.record(self.stream)
+            self.g.zero_()
+        stop.synchronize()
+        self.setup_seconds = start.elapsed_time(stop) / 1e3
+        self.sigma, self.tau, self.sigma_data = power_steps(self.algorithm, self.data_norm * NORM_MARGIN, sigma_data,
+                                                            data_share)
+        self.step_rule = "power"
 
     # ------------------------------------------------------------------ state
     def _alloc_state(self):
@@ -107,11 +196,12 @@ class PdhgSolver:
             setattr(st, name, ptr(getattr(self, name)))
         return st
 
-    def _params(self, sigma, tau) -> _lib.PdhgParams:
+    def _params(self, sigma, tau, sigma_data=None) -> _lib.PdhgParams:
         pr = _lib.PdhgParams()
         pr.algorithm = _lib.TR_ALG[self.algorithm]
         pr.l2_coupling = int(self.l2_coupling)
         pr.sigma, pr.tau = sigma, tau
+        pr.sigma_data = sigma if sigma_data is None else sigma_data
         pr.lam_m, pr.lam_e = self.lam["lam_m"], self.lam["lam_e"]
         pr.lam_w1, pr.lam_w2 = self.lam["lam_w1"], self.lam["lam_w2"]
         pr.use_graph = int(self.use_graph)
@@ -144,13 +234,18 @@ class PdhgSolver:
         return r
 
     # ------------------------------------------------------------------ iterate
-    def iterate(self, n_iter: int, tol: float = 0.0, sigma: float | None = None, tau: float | None = None):
-        """Run up to n_iter iterations from the current state; returns (iters, tols)."""
+    def iterate(self, n_iter: int, tol: float = 0.0, sigma: float | None = None, tau: float | None = None,
+                sigma_data: float | None = None):
+        """Run up to n_iter iterations from the current state; returns (iters, tols).
+        Steps default to the solver's (``sigma_data`` follows an explicit
+        ``sigma`` unless given)."""
         torch = self.torch
         hist = (ctypes.c_double * max(1, n_iter))()
         done = ctypes.c_int32(0)
+        if sigma_data is None:
+            sigma_data = self.sigma_data if sigma is None else sigma
         st, pr = self._state_struct(), self._params(self.sigma if sigma is None else sigma,
-                                                     self.tau if tau is None else tau)
+                                                     self.tau if tau is None else tau, sigma_data)
         self.stream.wait_stream(torch.cuda.current_stream(self.device))
         status = _lib.load().tr_pdhg_run(self.backend.plan, ctypes.byref(st), ctypes.byref(pr), int(n_iter),
                                          float(tol), hist, ctypes.byref(done),
@@ -162,23 +257,26 @@ class PdhgSolver:
     def run(self, max_iter: int = 300, tol: float = 1e-3, init: Optional[dict] = None) -> SolveResult:
         """``*Reconstructor.run`` on the device: reset, iterate, return u_bar."""
         torch = self.torch
-        sigma, tau = self.sigma, self.tau
+        sigma, tau, sigma_data = self.sigma, self.tau, self.sigma_data
         while True:
             self.reset(init)
             start = torch.cuda.Event(enable_timing=True)
             stop = torch.cuda.Event(enable_timing=True)
             try:
                 start.record(self.stream)
-                iters, tols = self.iterate(max_iter, tol, sigma, tau)
+                iters, tols = self.iterate(max_iter, tol, sigma, tau, sigma_data)
                 stop.record(self.stream)
                 stop.synchronize()
                 return SolveResult(image=self.u_bar, iterations=iters, tols=tols,
-                                   seconds=start.elapsed_time(stop) / 1e3, sigma=sigma, tau=tau)
+                                   seconds=start.elapsed_time(stop) / 1e3, sigma=sigma, tau=tau,
+                                   sigma_data=sigma_data, step_rule=self.step_rule, data_norm=self.data_norm,
+                                   setup_seconds=self.setup_seconds)
             except OverflowError:
                 if self.algorithm == "tvmw":   # the reference's TVMW has no retry
                     raise
                 sigma *= 0.9
                 tau *= 0.9
+                sigma_data *= 0.9
 
     def close(self):
         self.backend.close()

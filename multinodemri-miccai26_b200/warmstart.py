@@ -297,9 +297,11 @@ def warm_solve(solver, cfg=None, max_iter: int = 300, tol: float = 1e-3, model=N
 
 
 # ---------------------------------------------------------------------- training
-def make_pairs(n: int, base_cfg, device=0, max_iter: int = 300, tol: float = 1e-3, seed0: int = 1000):
+def make_pairs(n: int, base_cfg, device=0, max_iter: int = 300, tol: float = 1e-3, seed0: int = 1000,
+               step_rule: str = "reference"):
     """(x0, target) volumes from n seeded phantoms: x0 the density-compensated
-    adjoint, target the plain b200 PDHG result; both (n*B*E, Z, Y, X) complex64."""
+    adjoint, target the plain b200 PDHG result at (tol, max_iter) under
+    ``step_rule``; both (n*B*E, Z, Y, X) complex64."""
     import torch
     from dataclasses import replace
     from . import synthetic as syn
@@ -311,7 +313,7 @@ def make_pairs(n: int, base_cfg, device=0, max_iter: int = 300, tol: float = 1e-
         syn.simulate_kspace_b200(ds, device)
         s = PdhgSolver(cfg.algorithm, cfg.img_shape, [ds.coord[ds.bin_indices(b)] for b in range(cfg.n_bins)],
                        ds.bin_dcf(), ds.mps, ds.bin_ksp(), l2_coupling=cfg.l2_coupling, lam_m=cfg.lam,
-                       lam_e=cfg.lam, lam_w1=cfg.lam, lam_w2=cfg.lam, device=device)
+                       lam_e=cfg.lam, lam_w1=cfg.lam, lam_w2=cfg.lam, device=device, step_rule=step_rule)
         x0 = s.adjoint_image()
         r = s.run(max_iter=max_iter, tol=tol)
         scale = float(x0.abs().max()) or 1.0
@@ -366,7 +368,8 @@ def relative_error(net, x0, target, device="cuda", limit: int = 8) -> float:
 
 
 # ---------------------------------------------------------------------- evaluation
-def holdout_eval(net, cfg, seed: int, max_iter: int = 300, tol: float = 1e-3, ref_iter: int = 0, device=0) -> dict:
+def holdout_eval(net, cfg, seed: int, max_iter: int = 300, tol: float = 1e-3, ref_iter: int = 0, device=0,
+                 step_rule: str = "reference") -> dict:
     """Plain and warm-started solves of one unseen phantom to (tol, max_iter).
 
     With ref_iter > 0 a zero-start solve of ref_iter iterations (no stopping
@@ -380,13 +383,13 @@ def holdout_eval(net, cfg, seed: int, max_iter: int = 300, tol: float = 1e-3, re
     syn.simulate_kspace_b200(ds, device)
     s = PdhgSolver(hcfg.algorithm, hcfg.img_shape, [ds.coord[ds.bin_indices(b)] for b in range(hcfg.n_bins)],
                    ds.bin_dcf(), ds.mps, ds.bin_ksp(), l2_coupling=hcfg.l2_coupling, lam_m=hcfg.lam,
-                   lam_e=hcfg.lam, lam_w1=hcfg.lam, lam_w2=hcfg.lam, device=device)
+                   lam_e=hcfg.lam, lam_w1=hcfg.lam, lam_w2=hcfg.lam, device=device, step_rule=step_rule)
     rel = lambda a, b: float((a - b).norm() / b.norm().clamp_min(1e-30))
     plain = s.run(max_iter=max_iter, tol=tol)
     plain_img = plain.image.clone()
     net.eval()
     warm = warm_solve(s, hcfg, max_iter=max_iter, tol=tol, model=net)
-    out = {"workload": hcfg.name, "seed": seed, "plain_iterations": plain.iterations,
+    out = {"workload": hcfg.name, "seed": seed, "step_rule": step_rule, "plain_iterations": plain.iterations,
            "plain_seconds": plain.seconds, "plain_final_tol": plain.tols[-1] if plain.tols else None,
            "warm_iterations": warm.iterations, "warm_seconds": warm.seconds,
            "warm_final_tol": warm.tols[-1] if warm.tols else None,
@@ -428,6 +431,8 @@ def main(argv=None):
     ap.add_argument("--ref-iter", type=int, default=0, help="iterations of the fixed-point stand-in (0: none)")
     ap.add_argument("--eval", action="store_true", help="evaluate the network at --out; no training")
     ap.add_argument("--eval-config", default=None, help="workload of the held-out solve (default --config)")
+    ap.add_argument("--step-rule", choices=("reference", "power"), default="power",
+                    help="PDHG steps of the target and evaluation solves")
     ap.add_argument("--out", default=str(WEIGHTS))
     args = ap.parse_args(argv)
     cfg = syn.CONFIGS[args.config]
@@ -435,12 +440,14 @@ def main(argv=None):
     seed_eval = 1000 + args.phantoms + args.holdout + 7
     if args.eval:
         net = load_model(Path(args.out))
-        res = holdout_eval(net, ecfg, seed_eval, max_iter=args.max_iter, tol=ecfg.tol, ref_iter=args.ref_iter)
+        res = holdout_eval(net, ecfg, seed_eval, max_iter=args.max_iter, tol=ecfg.tol, ref_iter=args.ref_iter,
+                           step_rule=args.step_rule)
         print(json.dumps({"eval": res, "trained": {k: v for k, v in net.meta.items() if k != "loss_history"}}))
         return
     t_tol = cfg.tol if args.target_tol is None else args.target_tol
     t0 = time.perf_counter()
-    x0, tgt = make_pairs(args.phantoms + args.holdout, cfg, max_iter=args.target_iter, tol=t_tol)
+    x0, tgt = make_pairs(args.phantoms + args.holdout, cfg, max_iter=args.target_iter, tol=t_tol,
+                         step_rule=args.step_rule)
     t_pairs = time.perf_counter() - t0
     n_train = args.phantoms * cfg.n_bins * cfg.n_echoes
     net_cfg = NetConfig(widths=tuple(args.widths), levels=len(args.widths))
@@ -454,9 +461,9 @@ def main(argv=None):
             "params": count_params(net), "pairs_seconds": t_pairs, "train_seconds": info["seconds"],
             "rel_err_train": err_train, "rel_err_holdout": err_hold, "rel_err_holdout_scaled_adjoint": base_hold,
             "loss_history": info["history"],
-            "target": f"zero-start b200 PDHG, max_iter {args.target_iter}, tol {t_tol}"}
+            "target": f"zero-start b200 PDHG, {args.step_rule} step rule, max_iter {args.target_iter}, tol {t_tol}"}
     meta["holdout_solve"] = holdout_eval(net, ecfg, seed_eval, max_iter=args.max_iter, tol=ecfg.tol,
-                                         ref_iter=args.ref_iter)
+                                         ref_iter=args.ref_iter, step_rule=args.step_rule)
     save_model(net, Path(args.out), meta)
     print(json.dumps(meta))
 

@@ -186,10 +186,12 @@ def tvm_init(pb: Problem):
             "q": [np.zeros_like(k) for k in pb.ksp]}
 
 
-def tvm_iterate(pb: Problem, st, sigma, tau, lam, l2_coupling=False):
-    """One ``TvmReconstructor.pdhg`` step (tvm.py:227-380), default reduce mode."""
+def tvm_iterate(pb: Problem, st, sigma, tau, lam, l2_coupling=False, sigma_data=None):
+    """One ``TvmReconstructor.pdhg`` step (tvm.py:227-380), default reduce mode.
+    ``sigma_data`` (default: ``sigma``) is the data-dual step; the reference uses
+    one sigma for every dual."""
     u_old = st["u"].copy()
-    st["q"] = data_dual(pb, st["u_bar"], st["q"], sigma)
+    st["q"] = data_dual(pb, st["u_bar"], st["q"], sigma if sigma_data is None else sigma_data)
     p_m = st["p_m"] + sigma * motion_diff(st["u_bar"])
     p_m = prox_motion(p_m, lam, l2_coupling)
     g = data_grad(pb, st["q"])
@@ -216,11 +218,11 @@ def tvme_init(pb: Problem):
     return st
 
 
-def tvme_iterate(pb: Problem, st, sigma, tau, lam_m, lam_e, l2_coupling=False):
+def tvme_iterate(pb: Problem, st, sigma, tau, lam_m, lam_e, l2_coupling=False, sigma_data=None):
     """One ``TvmeReconstructor.pdhg`` step (tvme.py:208-482) on one device."""
     u_bar = st["u_bar"]
     u_old = st["u"].copy()
-    st["q"] = data_dual(pb, u_bar, st["q"], sigma)
+    st["q"] = data_dual(pb, u_bar, st["q"], sigma if sigma_data is None else sigma_data)
     p_m = st["p_m"] + sigma * motion_diff(u_bar)
     if not l2_coupling:
         p_m = p_m / np.maximum(1.0, np.abs(p_m) / lam_m)
@@ -279,7 +281,8 @@ def tvmw_init(pb: Problem):
             "p_w1": z.copy(), "p_w2": [None] * pb.B, "q": [np.zeros_like(k) for k in pb.ksp]}
 
 
-def tvmw_iterate(pb: Problem, st, sigma, tau, lam1, lam2, lam3, l2_coupling=False, wavelet="db6"):
+def tvmw_iterate(pb: Problem, st, sigma, tau, lam1, lam2, lam3, l2_coupling=False, wavelet="db6",
+                 sigma_data=None):
     """One ``TvmwReconstructor.pdhg`` step (tvmw.py:385-685) on one device."""
     u = st["u_bar"]                       # "primal_u" in the reference
     st["u_old"] = st["u_tmp"].copy()
@@ -288,7 +291,7 @@ def tvmw_iterate(pb: Problem, st, sigma, tau, lam1, lam2, lam3, l2_coupling=Fals
         if st["p_w2"][b] is None:
             st["p_w2"][b] = w2_zeros_like(w2)
         st["p_w2"][b] = w2_project(w2_axpy(st["p_w2"][b], sigma, w2), lam3)
-    st["q"] = data_dual(pb, u, st["q"], sigma)
+    st["q"] = data_dual(pb, u, st["q"], sigma if sigma_data is None else sigma_data)
     p_m = st["p_m"] + sigma * motion_diff(u)
     if not l2_coupling:
         p_m = p_m / np.maximum(1.0, np.abs(p_m) / lam1)
@@ -346,11 +349,13 @@ def _tol_w(u_new, u_prev):
 
 def run(algorithm: str, pb: Problem, *, sigma=1 / 6, tau=1 / 6, max_iter=300, tol=1e-3,
         lam_m=1e-5, lam_e=1e-5, lam1=1e-5, lam2=1e-5, lam3=1e-5, l2_coupling=False,
-        init=None, keep_state=False) -> RunResult:
+        init=None, keep_state=False, sigma_data=None) -> RunResult:
     """``*Reconstructor.run`` on one device; returns ``u_bar`` like the reference.
 
     ``init`` optionally overrides the zero initial state (used only to check
-    warm starts; the reference always starts from zeros).
+    warm starts; the reference always starts from zeros).  ``sigma_data``
+    gives the data dual its own step (block-diagonal steps; the reference has
+    one sigma).
     """
     pb.cast()
     alg = algorithm.lower()
@@ -370,17 +375,40 @@ def run(algorithm: str, pb: Problem, *, sigma=1 / 6, tau=1 / 6, max_iter=300, to
     for it in range(max_iter):
         if alg == "tvmw":
             prev = st["u_bar"].copy()
-            tvmw_iterate(pb, st, sigma, tau, lam1, lam2, lam3, l2_coupling)
+            tvmw_iterate(pb, st, sigma, tau, lam1, lam2, lam3, l2_coupling, sigma_data=sigma_data)
             t = _tol_w(st["u_bar"], prev)
         else:
             prev = st["u"].copy()
             if alg == "tvm":
-                tvm_iterate(pb, st, sigma, tau, lam_m, l2_coupling)
+                tvm_iterate(pb, st, sigma, tau, lam_m, l2_coupling, sigma_data=sigma_data)
             else:
-                tvme_iterate(pb, st, sigma, tau, lam_m, lam_e, l2_coupling)
+                tvme_iterate(pb, st, sigma, tau, lam_m, lam_e, l2_coupling, sigma_data=sigma_data)
             t = _tol_u(st["u"], prev)
         tols.append(t)
         it_done = it + 1
         if t < tol:
             break
     return RunResult(image=st["u_bar"], iterations=it_done, tols=tols, state=st if keep_state else None)
+
+
+# ---------------------------------------------------------------- step rule
+def power_norm(pb: Problem, n_iter: int = 30, seed: int = 0) -> float:
+    """sqrt(||A^H W A||) by power iteration in FP64, A = [F_b S_c] over every
+    bin, echo and coil and W the density weights: the data operator of the
+    PDHG loop (``data_grad(data_dual(.))`` without the prox).  The reference
+    has no such estimate (it fixes sigma = tau = 1/6, ``tvme.py:968``)."""
+    pb.cast()
+    rng = np.random.default_rng(seed)
+    shape = (pb.B, pb.E) + pb.img_shape
+    x = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    lam = 0.0
+    for _ in range(n_iter):
+        x = x / np.linalg.norm(x.ravel())
+        ksp = []
+        for b in range(pb.B):
+            img = x[b][:, None] * pb.mps[None]
+            ksp.append(pb.nufft.forward(img, b).astype(np.complex128))
+        x = data_grad(pb, ksp)
+        lam = float(np.linalg.norm(x.ravel()))
+    return math.sqrt(lam)
+
