@@ -99,6 +99,7 @@ def parse(argv=None):
     ap.add_argument("--step-rule", choices=("power", "reference"), default="power",
                     help="PDHG steps of the timed solves: block-diagonal steps from the FP64 power-iteration "
                          "norm estimate (default), or the reference's sigma = tau = 1/6")
+    ap.add_argument("--no-warm", action="store_true", help="skip the warm-started solve")
     ap.add_argument("--no-oracle-check", action="store_true",
                     help="skip the FP64-oracle error report on the small crop of the workload")
     return ap.parse_args(argv)
@@ -354,6 +355,8 @@ def run_b200(args):
     # ---- warm-started solve (learned initial iterate), when a trained network exists
     warm = None
     try:
+        if args.no_warm or cfg.algorithm != "tvme":
+            raise FileNotFoundError("not requested (the network is trained for TVME)")
         ws = importlib.import_module(f"{PKG}.warmstart")
         warm = ws.warm_solve(solver, cfg, max_iter=cfg.max_iter, tol=cfg.tol)
     except (ImportError, FileNotFoundError, AttributeError) as exc:
@@ -449,8 +452,8 @@ def run_b200(args):
                        "step_rule": args.step_rule,
                        "parallelism": "replicas" if world > 1 else "single-gpu"},
             "value_source": ("warm-started PDHG" if use_warm else "plain PDHG") + f", {args.step_rule} step rule",
-            "steps": {"sigma": r_plain.sigma, "tau": r_plain.tau, "sigma_data": r_plain.sigma_data,
-                      "data_norm": r_plain.data_norm, "norm_estimate_s": round(r_plain.setup_seconds, 4)},
+            "pdhg_steps": {"sigma": r_plain.sigma, "tau": r_plain.tau, "sigma_data": r_plain.sigma_data,
+                           "data_norm": r_plain.data_norm, "norm_estimate_s": round(r_plain.setup_seconds, 4)},
             "tol_reached_plain": bool(r_plain.tols and r_plain.tols[-1] < cfg.tol),
             "time_to_tol_plain_s": round(t_plain, 4),
             "iterations_plain": r_plain.iterations,

@@ -193,6 +193,11 @@ typedef struct {
  * phase 2: primal update, extrapolation and the FP64 tolerance sums
  *          (numerator, denominator) of the plan's bins into tol_sums[2]
  *          (device memory) for the caller's all-reduce; reads shard->p_m_prev.
+ * phase 3: the part of phase 1 that reads only this plan's state (TVMW
+ *          spatial-wavelet dual, data dual with its forward NUFFTs);
+ * phase 4: the rest of phase 1 (TV / W1 duals, data gradient); reads
+ *          shard->u_bar_next.  Phases 3 then 4 do exactly what phase 1 does,
+ *          so a caller can enqueue 3 while the u_bar halo is in flight.
  * Between the phases the caller passes its last p_m bin to the next rank; after
  * phase 2 its first u_bar bin to the previous rank.  TR_ERR_TIMEOUT reports a
  * device wait that expired in an earlier phase on this plan. */

@@ -381,7 +381,7 @@ __device__ __forceinline__ void fft_ct_ld(float2* A, float2* B, const float2* tw
 template <int L, int W, int NT, bool INV, int s, int Ns>
 struct CtStageIP {
     template <class Store>
-    __device__ __forceinline__ static void run(float2* buf, const float2* __restrict__ tw, Store& store, int tid) {
+    __device__ __forceinline__ static void run(float2* buf, const float2* __restrict__ tw, Store& store) {
         constexpr int S = ct_nstages(L);
         constexpr int R = ct_radix(L, s);
         constexpr int NB = L / R;
@@ -391,7 +391,7 @@ struct CtStageIP {
         float2 v[ITERS][R];
 #pragma unroll
         for (int it = 0; it < ITERS; ++it) {
-            const int idx = tid + it * NT;
+            const int idx = (int)threadIdx.x + it * NT;
             if (TOTAL % NT == 0 || idx < TOTAL) {
                 const int j = idx / W;
                 const int w = idx - j * W;
@@ -412,7 +412,7 @@ struct CtStageIP {
         __syncthreads();                                   // every read of this stage is done
 #pragma unroll
         for (int it = 0; it < ITERS; ++it) {
-            const int idx = tid + it * NT;
+            const int idx = (int)threadIdx.x + it * NT;
             if (TOTAL % NT == 0 || idx < TOTAL) {
                 const int j = idx / W;
                 const int w = idx - j * W;
@@ -427,17 +427,13 @@ struct CtStageIP {
         }
         if constexpr (s < S - 1) {
             __syncthreads();
-            CtStageIP<L, W, NT, INV, s + 1, Ns * R>::run(buf, tw, store, tid);
+            CtStageIP<L, W, NT, INV, s + 1, Ns * R>::run(buf, tw, store);
         }
     }
 };
-// tid: the calling thread's index in the CTA.  A caller that transforms several
-// tiles in a loop can pass a value the compiler cannot prove loop-invariant, so
-// the per-stage index arithmetic is recomputed per tile instead of being hoisted
-// out of the loop and held in registers across it.
 template <int L, int W, int NT, bool INV, class Store>
-__device__ __forceinline__ void fft_ct_ip(float2* buf, const float2* tw, Store& store, int tid = threadIdx.x) {
-    CtStageIP<L, W, NT, INV, 0, 1>::run(buf, tw, store, tid);
+__device__ __forceinline__ void fft_ct_ip(float2* buf, const float2* tw, Store& store) {
+    CtStageIP<L, W, NT, INV, 0, 1>::run(buf, tw, store);
 }
 
 // Buffer that the last stage of an L-point fft_ct does not read.

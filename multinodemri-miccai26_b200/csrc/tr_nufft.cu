@@ -26,7 +26,6 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
-#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -787,7 +786,8 @@ __global__ void __launch_bounds__(NT) k_fwd_x_tma(FwdXArgs a, const __grid_const
     const float apzy = s_apzy;
     const int h = a.h, pad = a.pad;
     const float* apx = a.apx;
-    // input element m of column w: u * S * apodisation * scale at x = (m + L/2) mod L - pad, 0 outside the image
+    // input element m of column w: u * S * apodisation * scale at x = (m + L/2) mod L - pad, 0 outside the
+    // image (scaling the image row once in shared memory first measured 1 % slower: one more barrier)
     auto load = [=](int m, int w) {
         int j = m + h;
         if (j >= L) j -= L;
@@ -809,9 +809,13 @@ __global__ void __launch_bounds__(NT) k_fwd_x_tma(FwdXArgs a, const __grid_const
     }
 }
 
-template <int L, int W, int NT = ct_threads(L, W)>
-__global__ void __launch_bounds__(NT, (W >= 16 || NT > 256 ? 3 : 4)) k_adj_x_tma(AdjXArgs a,
-                                                                                const __grid_constant__ CUtensorMap tin) {
+// PF: the coil maps of each group are loaded into registers before the
+// transform (in flight during it); otherwise in the epilogue.  MINB: CTAs per
+// SM the register allocation is sized for.  At L = 320, W = 8 the epilogue
+// loads with four CTAs per SM (48 registers) measured 4 % faster than the
+// prefetch with three (64 registers); the prefetch with four spills.
+template <int L, int W, int NT = ct_threads(L, W), bool PF = false, int MINB = 4>
+__global__ void __launch_bounds__(NT, MINB) k_adj_x_tma(AdjXArgs a, const __grid_constant__ CUtensorMap tin) {
     extern __shared__ __align__(128) unsigned char xsm_raw[];
     __shared__ __align__(8) uint64_t bar;
     float2* sm = align128(xsm_raw);
@@ -842,9 +846,9 @@ __global__ void __launch_bounds__(NT, (W >= 16 || NT > 256 ? 3 : 4)) k_adj_x_tma
     if (threadIdx.x == 0) issue(0);
     int phase = 0;
     for (int c0 = 0; c0 < a.C; c0 += W, phase ^= 1) {
-        // this column's W coil-map values, in flight during the transform
+        // this column's W coil-map values, in flight during the transform (PF)
         float4 m2[W / 2];
-        if (x < X) {
+        if (PF && x < X) {
 #pragma unroll
             for (int q = 0; q < W / 2; ++q) m2[q] = mrow[(c0 >> 1) + q];
         }
@@ -863,6 +867,10 @@ __global__ void __launch_bounds__(NT, (W >= 16 || NT > 256 ? 3 : 4)) k_adj_x_tma
         if (kEarly && threadIdx.x == 0 && c0 + W < a.C) issue(c0 + W);
         // conj(S) product and the sum over this group's coils, in coil order
         if (x < X) {
+            if (!PF) {
+#pragma unroll
+                for (int q = 0; q < W / 2; ++q) m2[q] = mrow[(c0 >> 1) + q];
+            }
 #pragma unroll
             for (int q = 0; q < W / 2; ++q) {
                 s = cadd(s, cmulc(ep[(2 * q) * XP + x], make_float2(m2[q].x, m2[q].y)));
@@ -881,100 +889,6 @@ __global__ void __launch_bounds__(NT, (W >= 16 || NT > 256 ? 3 : 4)) k_adj_x_tma
         if (a.accumulate) v = cadd(*dst, v);
         *dst = v;
     }
-}
-
-// In-place adjoint x pass: two [L][W] tiles, so the first two coil groups'
-// loads are in flight together and group g + 2 loads into the tile group g
-// has finished with; each tile is transformed in place (fft_ct_ip) and its
-// last stage writes the cropped rows over the same tile in [W][XP] order; the
-// coil maps are read from global memory (L2: the n_img CTAs of a row share
-// them) in the epilogue instead of being held in registers across the
-// transform.  Same butterflies, crop, coil order and sums as k_adj_x_tma (the
-// same bits), fewer registers, so five CTAs of 320 threads share an SM.
-template <int L, int W, int MINB, int NT = ct_threads(L, W)>
-__global__ void __launch_bounds__(NT, MINB) k_adj_x_tma2(AdjXArgs a, const __grid_constant__ CUtensorMap tin) {
-    extern __shared__ __align__(128) unsigned char xsm_raw[];
-    __shared__ __align__(8) uint64_t bar[2];
-    float2* sm = align128(xsm_raw);
-    float2* tws = sm + 2 * L * W;
-    const int X = a.X;                      // <= NT: thread x owns image column x
-    const int XP = X + 4;                   // padded row of the [W][XP] epilogue (X + 4 <= L)
-    const int img = (int)(blockIdx.x % (unsigned)a.n_img);
-    const int row = (int)(blockIdx.x / (unsigned)a.n_img);
-    const int x = threadIdx.x;
-    const int ngroups = a.C / W;
-    if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-    }
-    for (int i = threadIdx.x; i < L; i += NT) tws[i] = a.tw[i];
-    __syncthreads();                        // barriers initialised
-    auto issue = [&](int g) {
-        float2* t = sm + (g & 1) * (L * W);
-        uint64_t* b = &bar[g & 1];
-        mbar_expect_tx(b, (unsigned)(L * W * sizeof(float2)));
-        const int col = img * a.C + g * W;
-        tma_load_3d(t, &tin, b, col, L / 2, row);
-        tma_load_3d(t + (L / 2) * W, &tin, b, col, 0, row);
-    };
-    if (threadIdx.x == 0) {
-        issue(0);
-        if (ngroups > 1) issue(1);
-    }
-    const int shift = a.h - a.pad;
-    const float4* mrow = reinterpret_cast<const float4*>(a.maps + ((int64_t)row * X + x) * a.C);
-    float2 s = make_float2(0.f, 0.f);
-#pragma unroll 1
-    for (int g = 0; g < ngroups; ++g) {
-        float2* t = sm + (g & 1) * (L * W);
-        const bool ok = mbar_wait_or_drain(&bar[g & 1], (unsigned)((g >> 1) & 1), a.poll);
-        if (__syncthreads_or(!ok)) {
-            // the other tile's copy (group g + 1) is in flight too: let it land before leaving
-            if (g + 1 < ngroups) mbar_wait_bounded(&bar[(g + 1) & 1], (unsigned)(((g + 1) >> 1) & 1), kMbarDrainLimit);
-            if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
-            return;
-        }
-        float2* ep = t;
-        auto store = [ep, shift, X, XP](int k, int w, float2 v) {
-            int o = k + shift;
-            o = o >= L ? o - L : (o < 0 ? o + L : o);
-            if (o < X) ep[w * XP + o] = v;
-        };
-        int tid;                            // threadIdx.x, opaque to loop-invariant code motion
-        asm volatile("mov.u32 %0, %%tid.x;" : "=r"(tid));
-        fft_ct_ip<L, W, NT, true>(t, tws, store, tid);
-        __syncthreads();                    // ep complete
-        if (x < X) {
-#pragma unroll
-            for (int q = 0; q < W / 2; ++q) {
-                const float4 m = mrow[((g * W) >> 1) + q];
-                s = cadd(s, cmulc(ep[(2 * q) * XP + x], make_float2(m.x, m.y)));
-                s = cadd(s, cmulc(ep[(2 * q + 1) * XP + x], make_float2(m.z, m.w)));
-            }
-        }
-        if (g + 2 < ngroups) {
-            fence_proxy_async_smem();       // this tile's generic-proxy accesses before the next TMA write
-            __syncthreads();                // every read of ep is done: the tile is free
-            if (threadIdx.x == 0) issue(g + 2);
-        }
-    }
-    if (x < X) {
-        const int z = row / a.Y, y = row - z * a.Y;
-        float2 v = cscale(s, a.apz[z] * a.apy[y] * a.scale * a.apx[x]);
-        float2* dst = a.img + (int64_t)img * a.img_stride + (int64_t)row * X + x;
-        if (a.accumulate) v = cadd(*dst, v);
-        *dst = v;
-    }
-}
-
-// Kernel variants selected by TOPORECON_B200_KERNELS (comparison runs of the
-// variants kept during tuning); empty: the defaults.
-static bool kernel_variant(const char* name) {
-    static const std::string sel = [] {
-        const char* e = std::getenv("TOPORECON_B200_KERNELS");
-        return std::string(e ? e : "");
-    }();
-    return sel.find(name) != std::string::npos;
 }
 
 // ------------------------------------------------------------------ per-sample tap records
@@ -1107,7 +1021,9 @@ __global__ void __launch_bounds__(256) k_interp(const float2* __restrict__ grid,
 // trailing CTAs write zeros into tiles no sample reaches, kZeroTiles each.
 // k_spread_reduce then adds the partial tiles to the grid in range order.
 constexpr int kTile = 4;
-constexpr int kSpreadSub = 32;      // list entries staged per sub-chunk (= points of two z planes of a tile)
+// List entries staged per sub-chunk (= points of kSlabZ z planes of a tile);
+// 64 measured 6 % slower than 32 on the 96-column TVME-256 gridding.
+constexpr int kSpreadSub = 32;
 constexpr int kSlabZ = kSpreadSub / 16;            // z planes per staged piece of a finished tile
 static_assert(kSpreadSub % 16 == 0 && 64 % kSpreadSub == 0, "pieces of whole z planes");
 constexpr int kZeroTiles = 4;       // empty tiles per zero-fill CTA (plain stores)
@@ -1818,8 +1734,7 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
     if (p->use_tma && ct && maps && C % kTmaXWidth == 0 && OSX / 2 <= 256 && X <= 256 && X + 4 <= OSX) {
         CUtensorMap tin;
         const void* tfn = nullptr;
-        const int v2 = kernel_variant("adjx2") ? 4 : kernel_variant("adjx3") ? 5 : 0;
-#define TR_ADJX_TMA(LV) case LV: tfn = v2 == 4 ? (const void*)k_adj_x_tma2<LV, kTmaXWidth, 4> : v2 == 5 ? (const void*)k_adj_x_tma2<LV, kTmaXWidth, 5> : (const void*)k_adj_x_tma<LV, kTmaXWidth>; break;
+#define TR_ADJX_TMA(LV) case LV: tfn = (const void*)k_adj_x_tma<LV, kTmaXWidth>; break;
         switch (OSX) { TR_CT_LENGTHS(TR_ADJX_TMA) default: break; }
 #undef TR_ADJX_TMA
         if (tfn && encode_map_3d(&tin, p->bufA, (uint64_t)aa.ncol, (uint64_t)OSX, (uint64_t)Z * Y, (uint32_t)kTmaXWidth,

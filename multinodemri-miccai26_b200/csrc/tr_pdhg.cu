@@ -359,15 +359,17 @@ static PdArgs make_args(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_params
 }
 
 // Phase 1: every dual update and the data gradient (reads u_bar, u_bar_next).
-static tr_status enqueue_phase1(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_params* q, const ShardView& sh,
-                                cudaStream_t st) {
+// Phase 1 is enqueued in two parts: `local` (the TVMW spatial-wavelet dual and
+// the data dual; they read only this plan's u_bar) and `halo` (the TV / W1 duals,
+// which read u_bar_next, and the data gradient).  A sharded caller posts the
+// u_bar halo, enqueues the local part while it travels, then the halo part.
+static tr_status enqueue_phase1_local(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_params* q, cudaStream_t st) {
     const int64_t N = (int64_t)p->n[0] * p->n[1] * p->n[2];
     const int64_t EN = (int64_t)p->E * N;
     const int ncol = p->E * p->C;
     float2* ubar = (float2*)s->u_bar;
     float2* qd = (float2*)s->q;
     const float2* y = (const float2*)s->y;
-    float2* g = (float2*)s->g;
     // TVMW: the spatial-wavelet dual reads u_bar before anything changes it
     if (q->algorithm == TR_ALG_TVMW)
         TR_TRY(wavelet_dual(p, ubar, (float2*)s->p_w2, q->sigma, q->lam_w2, st));
@@ -378,6 +380,16 @@ static tr_status enqueue_phase1(tr_plan* p, const tr_pdhg_state* s, const tr_pdh
         TR_TRY(nufft_forward_cols(p, b, ubar + (int64_t)b * EN, N, p->E, p->maps, p->C, kInterpDualProx, sigma_data,
                                   y + off, qd + off, st));
     }
+    return TR_OK;
+}
+
+static tr_status enqueue_phase1_halo(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_params* q, const ShardView& sh,
+                                     cudaStream_t st) {
+    const int64_t N = (int64_t)p->n[0] * p->n[1] * p->n[2];
+    const int64_t EN = (int64_t)p->E * N;
+    const int ncol = p->E * p->C;
+    float2* qd = (float2*)s->q;
+    float2* g = (float2*)s->g;
     // 2. TV / W1 duals
     PdArgs a = make_args(p, s, q, sh);
     const unsigned blocks = (unsigned)(((int64_t)p->B * N + 255) / 256);
@@ -398,6 +410,12 @@ static tr_status enqueue_phase1(tr_plan* p, const tr_pdhg_state* s, const tr_pdh
     }
     if (q->algorithm == TR_ALG_TVMW) TR_TRY(wavelet_adjoint(p, (const float2*)s->p_w2, (float2*)s->w2adj, st));
     return TR_OK;
+}
+
+static tr_status enqueue_phase1(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_params* q, const ShardView& sh,
+                                cudaStream_t st) {
+    TR_TRY(enqueue_phase1_local(p, s, q, st));
+    return enqueue_phase1_halo(p, s, q, sh, st);
 }
 
 // Phase 2: primal update, extrapolation and the FP64 tolerance sums of the
@@ -525,12 +543,12 @@ extern "C" tr_status tr_pdhg_phase(tr_plan* plan, const tr_pdhg_state* state, co
                                    const tr_pdhg_shard* shard, int32_t phase, double* tol_sums, void* stream) {
     if (!plan || !shard) return fail(TR_ERR_INVALID_ARG, "tr_pdhg_phase: null argument");
     TR_TRY(validate(plan, state, params));
-    if (phase != 1 && phase != 2) return fail(TR_ERR_INVALID_ARG, "tr_pdhg_phase: phase must be 1 or 2");
+    if (phase < 1 || phase > 4) return fail(TR_ERR_INVALID_ARG, "tr_pdhg_phase: phase must be 1, 2, 3 or 4");
     if (shard->bin_offset < 0 || shard->n_bins_global < shard->bin_offset + plan->B)
         return fail(TR_ERR_INVALID_ARG, "tr_pdhg_phase: n_bins_global must cover bin_offset + the plan's bins");
     const bool has_next = shard->bin_offset + plan->B < shard->n_bins_global;
     const bool has_prev = shard->bin_offset > 0;
-    if (phase == 1 && has_next && !shard->u_bar_next)
+    if ((phase == 1 || phase == 4) && has_next && !shard->u_bar_next)
         return fail(TR_ERR_INVALID_ARG, "tr_pdhg_phase: u_bar_next is required unless the plan holds the last bin");
     if (phase == 2 && has_prev && !shard->p_m_prev)
         return fail(TR_ERR_INVALID_ARG, "tr_pdhg_phase: p_m_prev is required unless the plan holds the first bin");
@@ -554,6 +572,10 @@ extern "C" tr_status tr_pdhg_phase(tr_plan* plan, const tr_pdhg_state* state, co
     tr_status rc;
     if (phase == 1) {
         rc = enqueue_phase1(plan, state, params, sh, st);
+    } else if (phase == 3) {
+        rc = enqueue_phase1_local(plan, state, params, st);
+    } else if (phase == 4) {
+        rc = enqueue_phase1_halo(plan, state, params, sh, st);
     } else {
         rc = enqueue_phase2(plan, state, params, sh, tol_sums, st);
         if (rc == TR_OK && cudaMemcpyAsync(plan->err_host, plan->dev_err, sizeof(int), cudaMemcpyDeviceToHost, st) !=

@@ -7,8 +7,12 @@ one-bin ghosts around the motion TV (``tvme.py:217-229`` sends u_bar forward,
 stopping sums (``tvme.py:518-551``).  Here every rank holds a contiguous range
 of motion bins (all echoes and coils of them) in one plan; an iteration is
 
-    u_bar halo   first local u_bar bin -> previous rank (its ``u_bar_next``)
-    phase 1      data dual, TV / wavelet duals, data gradient   (tr_pdhg_phase)
+    u_bar halo   first local u_bar bin -> previous rank (its ``u_bar_next``),
+                 posted without waiting
+    phase 1a     data dual (forward NUFFTs), TVMW wavelet dual: local state only,
+                 so it runs while the halo travels           (tr_pdhg_phase 3)
+    (wait for the u_bar halo)
+    phase 1b     TV / W1 duals, data gradient                (tr_pdhg_phase 4)
     p_m halo     last local p_m bin -> next rank (its ``p_m_prev``)
     phase 2      primal update, extrapolation, local FP64 stopping sums
     all-reduce   of the two sums; every rank takes the same stopping decision
@@ -91,16 +95,27 @@ class TorchHaloComm:
         self.world = dist.get_world_size(group)
         self.prev, self.next = neighbours(ranges, self.rank)
 
-    def _exchange(self, send, send_to, recv, recv_from):
+    def _post(self, send, send_to, recv, recv_from):
         dist = self.dist
         ops = []
         if send_to is not None:
             ops.append(dist.P2POp(dist.isend, send, send_to, self.group))
         if recv_from is not None:
             ops.append(dist.P2POp(dist.irecv, recv, recv_from, self.group))
-        if ops:
-            for w in dist.batch_isend_irecv(ops):
-                w.wait()
+        return dist.batch_isend_irecv(ops) if ops else []
+
+    def _exchange(self, send, send_to, recv, recv_from):
+        self.wait(self._post(send, send_to, recv, recv_from))
+
+    @staticmethod
+    def wait(works):
+        """Complete posted transfers (with NCCL: the current stream waits for them)."""
+        for w in works:
+            w.wait()
+
+    def post_backward(self, first_bin, halo_next):
+        """Start ``pass_backward`` and return its handle for ``wait``."""
+        return self._post(first_bin, self.prev, halo_next, self.next)
 
     def pass_backward(self, first_bin, halo_next):
         """Send this rank's first bin to the previous rank; receive the next
@@ -149,8 +164,10 @@ class ShardedPdhg:
         eng, comm = self.engine, self.comm
         tols = []
         for _ in range(n_iter):
-            comm.pass_backward(eng.first_u_bar(), eng.u_bar_next)
-            eng.phase1(sigma, tau)
+            halo = comm.post_backward(eng.first_u_bar(), eng.u_bar_next)
+            eng.phase1a(sigma, tau)                  # overlaps the u_bar halo
+            comm.wait(halo)
+            eng.phase1b(sigma, tau)
             comm.pass_forward(eng.last_p_m(), eng.p_m_prev)
             sums = eng.phase2(sigma, tau)
             comm.all_reduce_sum(sums)
@@ -255,6 +272,12 @@ class B200ShardEngine:
     def phase1(self, sigma, tau):
         self._phase(1, sigma, tau)
 
+    def phase1a(self, sigma, tau):
+        self._phase(3, sigma, tau)
+
+    def phase1b(self, sigma, tau):
+        self._phase(4, sigma, tau)
+
     def phase2(self, sigma, tau):
         self._phase(2, sigma, tau)
         self._to_current()
@@ -290,6 +313,12 @@ class IdleEngine:
         return _EventTimer(self.torch, self.torch.cuda.current_stream(self.device))
 
     def phase1(self, sigma, tau):
+        pass
+
+    def phase1a(self, sigma, tau):
+        pass
+
+    def phase1b(self, sigma, tau):
         pass
 
     def phase2(self, sigma, tau):

@@ -66,6 +66,11 @@ class OracleShardEngine:
 
     # ------------------------------------------------------------------ phases
     def phase1(self, sigma, tau):
+        self.phase1a(sigma, tau)
+        self.phase1b(sigma, tau)
+
+    def phase1a(self, sigma, tau):
+        """The part of phase 1 that reads only this rank's state."""
         pb, st, lam = self.pb, self.st, self.lam
         ub = st["u_bar"]
         if self.alg == "tvmw":
@@ -75,6 +80,11 @@ class OracleShardEngine:
                     st["p_w2"][b] = op.w2_zeros_like(w2)
                 st["p_w2"][b] = op.w2_project(op.w2_axpy(st["p_w2"][b], sigma, w2), lam)
         st["q"] = op.data_dual(pb, ub, st["q"], sigma)
+
+    def phase1b(self, sigma, tau):
+        """The rest of phase 1: it reads the next rank's first u_bar bin."""
+        pb, st, lam = self.pb, self.st, self.lam
+        ub = st["u_bar"]
         # motion forward difference with the next rank's first bin as ghost
         d = np.zeros_like(ub)
         if pb.B > 1:
@@ -168,6 +178,12 @@ class IdleEngine:
         pass
 
     def phase1(self, sigma, tau):
+        pass
+
+    def phase1a(self, sigma, tau):
+        pass
+
+    def phase1b(self, sigma, tau):
         pass
 
     def phase2(self, sigma, tau):
