@@ -70,6 +70,8 @@ typedef struct {
 
 #define TR_PLAN_AUTOTUNE 1       /* time candidate launch shapes at plan creation */
 #define TR_PLAN_NO_TMA 2         /* stage FFT tiles with cp.async instead of TMA (comparison runs) */
+#define TR_PLAN_YZ_FUSION 4      /* run the y and z FFT passes as one cluster kernel where the geometry
+                                    allows (comparison runs: measured slower than the separate passes) */
 
 typedef struct {
     int32_t os_shape[3];         /* oversampled grid (ceil(1.25 n) per axis) */
@@ -228,8 +230,11 @@ tr_status tr_wavelet_forward(tr_plan* plan, const void* images, void* coeffs, vo
 tr_status tr_wavelet_adjoint(tr_plan* plan, const void* coeffs, void* images, void* stream);
 
 /* Per-stage device time of the batched NUFFT of one bin (all E x C columns):
- * ms[8] and the algorithmic bytes[8] of each stage, in the order
- * forward x, y, z, interpolation(+dual prox), gridding, adjoint z, y, x.
+ * ms[10] and the algorithmic bytes[10] of each stage, in the order
+ * forward x, y, z, interpolation(+dual prox), gridding, adjoint z, y, x,
+ * fused forward y + z, fused adjoint z + y.  The last two are 0 ms / 0 bytes
+ * when the plan runs the separate passes; when it fuses them, the separate y
+ * and z passes are still timed for comparison.
  * Each stage is run reps times after one warm-up; used for roofline reports.
  * Replaces the reference's wall-clock timers (tvme.py:509, :561-567). */
 tr_status tr_profile_nufft(tr_plan* plan, int32_t bin, int32_t reps, double* ms, double* bytes, void* stream);

@@ -39,6 +39,10 @@ __device__ __forceinline__ void cp_async_wait_all() {
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
+// First 128-byte boundary at or after p (TMA boxes start there; launches add 128 bytes of slack).
+__device__ __forceinline__ float2* align128(unsigned char* p) {
+    return reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(p) + 127) & ~uintptr_t(127));
+}
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -78,6 +82,13 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, uint64_
         ::"r"(smem_u32(dst)), "l"(tmap), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
         : "memory");
 }
+__device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, uint64_t* bar, int c0, int c1, int c2,
+                                            int c3) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];\n"
+        ::"r"(smem_u32(dst)), "l"(tmap), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
+}
 __device__ __forceinline__ void tma_store_3d(const void* tmap, const void* src, int x, int y, int z) {
     asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4}], [%1];\n"
                  ::"l"(tmap), "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
@@ -101,6 +112,50 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 __device__ __forceinline__ void tma_store_commit_and_drain() {
     asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
     asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+}
+__device__ __forceinline__ void tma_store_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+// the issuing thread: every committed store group but the newest N has read its shared memory
+template <int N>
+__device__ __forceinline__ void tma_store_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read %0;\n" ::"n"(N) : "memory");
+}
+
+// ------------------------------------------------------------------ thread-block clusters
+// Distributed shared memory between the CTAs of a cluster (no TMA multicast).
+__device__ __forceinline__ unsigned cluster_rank() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ unsigned cluster_size() {
+    unsigned n;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(n));
+    return n;
+}
+// The address that `local` (this CTA's shared memory) has in CTA `rank` of the cluster.
+__device__ __forceinline__ unsigned dsmem_addr(const void* local, unsigned rank) {
+    unsigned remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(smem_u32(local)), "r"(rank));
+    return remote;
+}
+__device__ __forceinline__ float4 dsmem_load4(const void* local, unsigned rank) {
+    float4 v;
+    asm volatile("ld.shared::cluster.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "r"(dsmem_addr(local, rank))
+                 : "memory");
+    return v;
+}
+__device__ __forceinline__ void dsmem_store4(void* local, unsigned rank, float4 v) {
+    asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(dsmem_addr(local, rank)), "f"(v.x),
+                 "f"(v.y), "f"(v.z), "f"(v.w)
+                 : "memory");
+}
+// Every thread of every CTA of the cluster: shared-memory stores (local or
+// remote) before it are visible to loads after it.  A hardware barrier: the
+// CTAs of a cluster are scheduled together.
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
 // -i * z
@@ -378,7 +433,9 @@ __device__ __forceinline__ void fft_ct_ld(float2* A, float2* B, const float2* tw
 // [L][W] buffer; the last stage hands its outputs to store(k, w, v), which may
 // write into the buffer.  Same butterflies, twiddles and output order as
 // fft_ct (bit-identical results) with half the shared memory.
-template <int L, int W, int NT, bool INV, int s, int Ns>
+// RS: row stride of the buffer in elements (the W transformed columns are the
+// first W of each row; RS > W transforms a column subset of a wider tile).
+template <int L, int W, int NT, bool INV, int s, int Ns, int RS = W>
 struct CtStageIP {
     template <class Store>
     __device__ __forceinline__ static void run(float2* buf, const float2* __restrict__ tw, Store& store) {
@@ -398,7 +455,7 @@ struct CtStageIP {
                 const int k = (Ns == 1) ? 0 : j % Ns;
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    float2 x = buf[(j + r * NB) * W + w];
+                    float2 x = buf[(j + r * NB) * RS + w];
                     if (Ns > 1 && r > 0) {
                         float2 t = tw[k * r * STEP];
                         if (INV) t.y = -t.y;
@@ -421,19 +478,24 @@ struct CtStageIP {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     if (s == S - 1) store(d0 + r * Ns, w, v[it][r]);
-                    else buf[(d0 + r * Ns) * W + w] = v[it][r];
+                    else buf[(d0 + r * Ns) * RS + w] = v[it][r];
                 }
             }
         }
         if constexpr (s < S - 1) {
             __syncthreads();
-            CtStageIP<L, W, NT, INV, s + 1, Ns * R>::run(buf, tw, store);
+            CtStageIP<L, W, NT, INV, s + 1, Ns * R, RS>::run(buf, tw, store);
         }
     }
 };
 template <int L, int W, int NT, bool INV, class Store>
 __device__ __forceinline__ void fft_ct_ip(float2* buf, const float2* tw, Store& store) {
     CtStageIP<L, W, NT, INV, 0, 1>::run(buf, tw, store);
+}
+// The same on the first W columns of an [L][RS] buffer.
+template <int L, int W, int RS, int NT, bool INV, class Store>
+__device__ __forceinline__ void fft_ct_ip_rs(float2* buf, const float2* tw, Store& store) {
+    CtStageIP<L, W, NT, INV, 0, 1, RS>::run(buf, tw, store);
 }
 
 // Buffer that the last stage of an L-point fft_ct does not read.

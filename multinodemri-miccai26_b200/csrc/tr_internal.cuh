@@ -54,6 +54,7 @@ struct DeviceGuard {
 constexpr int kMbarPollLimit = 1 << 20;
 constexpr int kMbarDrainLimit = 1 << 20;
 constexpr int kDevErrTmaWait = 1;
+constexpr int kDevErrCluster = 2;   // a cluster kernel ran without the cluster shape it needs (no work done)
 
 // ------------------------------------------------------------------ complex helpers
 __host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
@@ -218,6 +219,7 @@ struct tr_plan {
     int line_width = 16;
     int spread_cols = 128;       // most k-space columns per gridding CTA
     bool use_tma = true;
+    bool fuse_yz = false;        // TR_PLAN_YZ_FUSION: fused y + z passes where the geometry allows
     bool autotune = false;       // TR_PLAN_AUTOTUNE: time launch-shape candidates on first use
     std::map<int, int> spread_cols_tuned;   // column count -> chosen spread_cols         // TMA-tiled FFT passes where the geometry allows
     // TVMW

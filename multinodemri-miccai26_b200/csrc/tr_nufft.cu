@@ -478,6 +478,224 @@ __global__ void __launch_bounds__(NT, (NT == 320 ? 5 : 6))
     }
 }
 
+// ------------------------------------------------------------------ fused y + z passes
+// The y and z passes of the forward (and the z and y passes of the adjoint)
+// in one kernel, so the intermediate (Z, OSY, OSX, ncol) volume never reaches
+// HBM.  A thread-block cluster of CL CTAs owns one x column and kYzCW
+// k-space columns, i.e. one (z, y) plane of kYzCW columns:
+//   forward   CTA r loads the image rows z in [r ZR, r ZR + ZR) of its plane
+//             (one 4-D TMA box per half, the y-centring rotation and the zero
+//             pad done by the TMA unit as in k_line_tma), transforms them along
+//             y in place ([LY][RS] tile, RS = ZR kYzCW), then after a cluster
+//             barrier takes the output rows y' in [r YR, r YR + YR): for two y'
+//             at a time it gathers the 8 lines' Z inputs from the CTAs holding
+//             them (distributed shared memory), transforms along z in place and
+//             stores the LZ grid rows by TMA (two boxes: the centring rotation);
+//   adjoint   the mirror image: z transforms of its y' rows (TMA loads, two
+//             chunks in flight), the Z cropped rows scattered to the CTAs that
+//             own them, a cluster barrier, then y transforms of its ZR rows and
+//             the Y cropped rows stored by TMA.
+// Each line sees exactly the butterflies, twiddles and order of k_line_tma, so
+// the results equal the separate passes bit for bit.  Reads of the plane all
+// precede the cluster barrier and writes follow it, so the grid can overwrite
+// the x-pass output of the same plane in place (other clusters touch other
+// (x, column) planes only).  No TMA multicast: every copy is between global
+// memory and the issuing CTA's own shared memory.
+// Measured on the 256 x 256 x 128 workload (96 columns, one B200): 17.5 ms
+// forward and 16.3 ms adjoint, against 7.7 and 7.5 ms for the separate passes.
+// Each cluster walks its plane as one serial chain (TMA load, y transforms,
+// cluster barrier, ten gather / transform / store rounds) at two CTAs per SM,
+// so the HBM round trip it saves does not pay; plans run these kernels only
+// with TR_PLAN_YZ_FUSION (comparison runs).
+constexpr int kYzCW = 4;      // k-space columns per cluster (32-byte rows)
+constexpr int kYzNT = 320;    // threads per CTA
+
+struct YzArgs {
+    int Z, Y;                 // image lengths along z and y
+    int pad_z, pad_y;         // centred zero-pad offsets (L / 2 - n / 2)
+    int ncol;
+    const float2* twz;        // [LZ] exp(-2 pi i k / LZ)
+    const float2* twy;        // [LY]
+    int* err;
+    int poll;
+};
+
+__host__ __device__ constexpr size_t yz_smem_bytes(int LY, int LZ, int ZR) {
+    return ((size_t)LY * ZR * kYzCW + 2 * (size_t)LZ * 8 + LY + LZ) * sizeof(float2) + 128;
+}
+
+template <int LY, int LZ, int CL, int ZR>
+__global__ void __launch_bounds__(kYzNT, 2) k_yz_fwd(YzArgs a, const __grid_constant__ CUtensorMap tin,
+                                                    const __grid_constant__ CUtensorMap tout) {
+    constexpr int CW = kYzCW, RS = ZR * CW, NT = kYzNT;
+    constexpr int YR = ((LY + CL - 1) / CL + 1) / 2 * 2;     // output rows y' per CTA (even)
+    static_assert(RS % 16 == 0 && LY % 2 == 0 && LZ % 2 == 0, "fused y/z tile shape");
+    extern __shared__ __align__(128) unsigned char yz_raw[];
+    __shared__ __align__(8) uint64_t bar;
+    float2* ty = align128(yz_raw);          // [LY][RS]: y lines of the CTA's ZR image rows
+    float2* tz = ty + LY * RS;              // [2][LZ][8]: z lines of two y' rows (two buffers)
+    float2* twy = tz + 2 * LZ * 8;
+    float2* twz = twy + LY;
+    if (cluster_size() != (unsigned)CL) {  // launched without its cluster: touch no other CTA
+        if (threadIdx.x == 0) atomicOr(a.err, kDevErrCluster);
+        return;
+    }
+    const unsigned r = cluster_rank();
+    const int cl = (int)(blockIdx.x / (unsigned)CL);
+    const int ncg = a.ncol / CW;
+    const int x = cl / ncg, c0 = (cl - x * ncg) * CW;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    for (int i = threadIdx.x; i < LY; i += NT) twy[i] = a.twy[i];
+    for (int i = threadIdx.x; i < LZ; i += NT) twz[i] = a.twz[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(&bar, (unsigned)(LY * RS * sizeof(float2)));
+        tma_load_4d(ty, &tin, &bar, c0, (int)r * ZR, LY / 2 - a.pad_y, x);
+        tma_load_4d(ty + (LY / 2) * RS, &tin, &bar, c0, (int)r * ZR, -a.pad_y, x);
+    }
+    const bool ok = mbar_wait_or_drain(&bar, 0, a.poll);
+    const bool bad = __syncthreads_or(!ok);
+    if (bad) {
+        if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
+    } else {
+#pragma unroll 1
+        for (int sub = 0; sub < RS / 16; ++sub) {
+            float2* b = ty + sub * 16;
+            auto store = [b](int k, int w, float2 v) { b[k * RS + w] = v; };
+            fft_ct_ip_rs<LY, 16, RS, NT, false>(b, twy, store);
+        }
+    }
+    cluster_sync_all();                     // every y line of the plane is transformed
+    const int y_lo = (int)r * YR, y_hi = min(y_lo + YR, LY);
+#pragma unroll 1
+    for (int i = 0, y0 = y_lo; y0 < y_hi; ++i, y0 += 2) {
+        float2* t = tz + (i & 1) * (LZ * 8);
+        if (i >= 2) {                       // this buffer's store from two chunks ago has read it
+            if (threadIdx.x == 0) tma_store_wait_read<1>();
+            __syncthreads();
+        }
+        // row k of the z line holds image row z = ((k + LZ/2) mod LZ) - pad_z (zero outside [0, Z));
+        // column (yl, c) is y' = y0 + yl, k-space column c0 + c
+        for (int idx = threadIdx.x; idx < LZ * 4; idx += NT) {
+            const int k = idx >> 2, yl = (idx >> 1) & 1, hf = idx & 1;
+            int z = k + LZ / 2;
+            if (z >= LZ) z -= LZ;
+            z -= a.pad_z;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (z >= 0 && z < a.Z) {
+                const int q = z / ZR, zl = z - q * ZR;
+                int ky = y0 + yl + LY / 2;  // y-transform row of output y' (centring rotation)
+                if (ky >= LY) ky -= LY;
+                v = dsmem_load4(ty + ky * RS + zl * CW + hf * 2, (unsigned)q);
+            }
+            reinterpret_cast<float4*>(t)[idx] = v;              // t[k][yl * 4 + hf * 2 .. + 1]
+        }
+        __syncthreads();
+        auto store = [t](int k, int w, float2 v) { t[k * 8 + w] = v; };
+        fft_ct_ip<LZ, 8, NT, false>(t, twz, store);
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0 && !bad) {
+            tma_store_4d(&tout, t + (LZ / 2) * 8, c0, y0, 0, x);   // z' in [0, LZ/2): rows [LZ/2, LZ)
+            tma_store_4d(&tout, t, c0, y0, LZ / 2, x);             // z' in [LZ/2, LZ): rows [0, LZ/2)
+            tma_store_commit();
+        }
+    }
+    if (threadIdx.x == 0) tma_store_wait_read<0>();
+    cluster_sync_all();                     // no CTA leaves while another still reads its y tile
+}
+
+template <int LY, int LZ, int CL, int ZR>
+__global__ void __launch_bounds__(kYzNT, 2) k_yz_adj(YzArgs a, const __grid_constant__ CUtensorMap tin,
+                                                    const __grid_constant__ CUtensorMap tout) {
+    constexpr int CW = kYzCW, RS = ZR * CW, NT = kYzNT;
+    constexpr int YR = ((LY + CL - 1) / CL + 1) / 2 * 2;
+    static_assert(RS % 16 == 0 && LY % 2 == 0 && LZ % 2 == 0, "fused y/z tile shape");
+    extern __shared__ __align__(128) unsigned char yz_raw[];
+    __shared__ __align__(8) uint64_t bar[2];
+    float2* ty = align128(yz_raw);          // [LY][RS]: y lines of the CTA's ZR output rows
+    float2* tz = ty + LY * RS;              // [2][LZ][8]
+    float2* twy = tz + 2 * LZ * 8;
+    float2* twz = twy + LY;
+    if (cluster_size() != (unsigned)CL) {  // launched without its cluster: touch no other CTA
+        if (threadIdx.x == 0) atomicOr(a.err, kDevErrCluster);
+        return;
+    }
+    const unsigned r = cluster_rank();
+    const int cl = (int)(blockIdx.x / (unsigned)CL);
+    const int ncg = a.ncol / CW;
+    const int x = cl / ncg, c0 = (cl - x * ncg) * CW;
+    const int y_lo = (int)r * YR, y_hi = min(y_lo + YR, LY);
+    const int nchunk = y_hi > y_lo ? (y_hi - y_lo) / 2 : 0;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+    }
+    for (int i = threadIdx.x; i < LY; i += NT) twy[i] = a.twy[i];
+    for (int i = threadIdx.x; i < LZ; i += NT) twz[i] = a.twz[i];
+    __syncthreads();
+    // grid rows z' of two y' rows: transform row k holds z' = (k + LZ/2) mod LZ
+    auto issue = [&](int i) {
+        float2* t = tz + (i & 1) * (LZ * 8);
+        mbar_expect_tx(&bar[i & 1], (unsigned)(LZ * 8 * sizeof(float2)));
+        tma_load_4d(t, &tin, &bar[i & 1], c0, y_lo + 2 * i, LZ / 2, x);
+        tma_load_4d(t + (LZ / 2) * 8, &tin, &bar[i & 1], c0, y_lo + 2 * i, 0, x);
+    };
+    if (threadIdx.x == 0) {
+        if (nchunk > 0) issue(0);
+        if (nchunk > 1) issue(1);
+    }
+    bool bad = false;
+#pragma unroll 1
+    for (int i = 0; i < nchunk; ++i) {
+        float2* t = tz + (i & 1) * (LZ * 8);
+        const bool ok = mbar_wait_or_drain(&bar[i & 1], (unsigned)((i >> 1) & 1), a.poll);
+        if (__syncthreads_or(!ok)) {
+            // the other buffer's copy may be in flight: let it land, then stop loading
+            if (i + 1 < nchunk)
+                mbar_wait_bounded(&bar[(i + 1) & 1], (unsigned)(((i + 1) >> 1) & 1), kMbarDrainLimit);
+            if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
+            bad = true;
+            break;
+        }
+        auto store = [t](int k, int w, float2 v) { t[k * 8 + w] = v; };
+        fft_ct_ip<LZ, 8, NT, true>(t, twz, store);
+        __syncthreads();
+        // output row z (cropped) is transform row (z - Z/2) mod LZ; it belongs to CTA z / ZR, whose
+        // y-transform row for y' = y_lo + 2 i + yl is (y' + LY/2) mod LY
+        for (int idx = threadIdx.x; idx < a.Z * 4; idx += NT) {
+            const int z = idx >> 2, yl = (idx >> 1) & 1, hf = idx & 1;
+            int kz = z - a.Z / 2;
+            if (kz < 0) kz += LZ;
+            const float4 v = reinterpret_cast<const float4*>(t)[kz * 4 + yl * 2 + hf];
+            const int q = z / ZR, zl = z - q * ZR;
+            int ky = y_lo + 2 * i + yl + LY / 2;
+            if (ky >= LY) ky -= LY;
+            dsmem_store4(ty + ky * RS + zl * CW + hf * 2, (unsigned)q, v);
+        }
+        fence_proxy_async_smem();           // generic reads of t before the next TMA write into it
+        __syncthreads();
+        if (threadIdx.x == 0 && i + 2 < nchunk) issue(i + 2);
+    }
+    cluster_sync_all();                     // every z-transformed row has reached its owner
+    if (!bad) {
+#pragma unroll 1
+        for (int sub = 0; sub < RS / 16; ++sub) {
+            float2* b = ty + sub * 16;
+            auto store = [b](int k, int w, float2 v) { b[k * RS + w] = v; };
+            fft_ct_ip_rs<LY, 16, RS, NT, true>(b, twy, store);
+        }
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0 && !bad) {
+        // output y in [0, Y/2): transform rows [LY - Y/2, LY); y in [Y/2, Y): rows [0, Y/2)
+        tma_store_4d(&tout, ty + (LY - a.Y / 2) * RS, c0, (int)r * ZR, 0, x);
+        tma_store_4d(&tout, ty, c0, (int)r * ZR, a.Y / 2, x);
+        tma_store_commit_and_drain();
+    }
+}
+
 template <int L, int W>
 __global__ void __launch_bounds__(256) k_fwd_x_ct(FwdXArgs a) {
     extern __shared__ float2 sm[];
@@ -747,9 +965,6 @@ __global__ void __launch_bounds__(256) k_adj_x_st(AdjXArgs a) {
 // writes the cropped row into shared memory, and the conj(S) product and the
 // coil sum run as in k_adj_x_st.  Loads complete on one mbarrier (phase per
 // coil group) with a bounded wait.
-__device__ __forceinline__ float2* align128(unsigned char* p) {
-    return reinterpret_cast<float2*>((reinterpret_cast<uintptr_t>(p) + 127) & ~uintptr_t(127));
-}
 
 template <int L, int W, int NT = 256>
 __global__ void __launch_bounds__(NT) k_fwd_x_tma(FwdXArgs a, const __grid_constant__ CUtensorMap timg,
@@ -1566,6 +1781,97 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
     return TR_OK;
 }
 
+// ---- fused y + z passes (k_yz_fwd / k_yz_adj)
+// 4-D map over complex64 data with dims (d0 contiguous, then d1, d2, d3 with
+// the given byte strides, in any order) and box [b3][b2][b1][b0].
+static bool encode_map_4d(CUtensorMap* m, const void* base, const uint64_t dims[4], const uint64_t strides[3],
+                          const uint32_t box[4]) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || ((uintptr_t)base & 15) || (box[0] * 8) % 16) return false;
+    for (int i = 0; i < 4; ++i)
+        if (box[i] < 1 || box[i] > 256 || box[i] > dims[i]) return false;
+    for (int i = 0; i < 3; ++i)
+        if (strides[i] % 16 || strides[i] >= (1ULL << 40)) return false;
+    const cuuint64_t d[4] = {dims[0], dims[1], dims[2], dims[3]};
+    const cuuint64_t s[3] = {strides[0], strides[1], strides[2]};
+    const cuuint32_t b[4] = {box[0], box[1], box[2], box[3]};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_INT64, 4, const_cast<void*>(base), d, s, b, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The compiled fused shapes: (LY, LZ, cluster size, image rows per CTA): the
+// 256 x 256 x 128 and 128 x 128 x 96 workloads' grids.
+#define TR_YZ_SHAPES(X) X(320, 160, 16, 8) X(160, 120, 8, 12)
+
+// Fused launch of the forward y + z (adj = false) or adjoint z + y passes on
+// plan buffer A in place; *done = false (nothing launched) when the plan, the
+// geometry or the device does not allow it, and the caller runs the separate
+// passes.
+static tr_status stage_yz(tr_plan* p, int ncol, bool adj, cudaStream_t st, bool* done) {
+    *done = false;
+    const int Z = p->n[0], Y = p->n[1], OSZ = p->os[0], OSY = p->os[1], OSX = p->os[2];
+    if (!p->use_tma || !p->fuse_yz || ncol % kYzCW || Z % 2 || Y % 2 || Y / 2 > 256) return TR_OK;
+    const void* fn = nullptr;
+    int CL = 0, ZR = 0;
+#define TR_YZ_PICK(LY, LZ, CLV, ZRV)                                                                   \
+    if (!fn && OSY == LY && OSZ == LZ && Z == CLV * ZRV) {                                             \
+        fn = adj ? (const void*)k_yz_adj<LY, LZ, CLV, ZRV> : (const void*)k_yz_fwd<LY, LZ, CLV, ZRV>;   \
+        CL = CLV;                                                                                      \
+        ZR = ZRV;                                                                                      \
+    }
+    TR_YZ_SHAPES(TR_YZ_PICK)
+#undef TR_YZ_PICK
+    if (!fn) return TR_OK;
+    const uint64_t n8 = (uint64_t)ncol * 8;
+    // image-side volume (Z, Y, OSX, ncol) viewed as (c, z, y, x); grid (OSZ, OSY, OSX, ncol) as (c, y, z, x)
+    const uint64_t img_dims[4] = {(uint64_t)ncol, (uint64_t)Z, (uint64_t)Y, (uint64_t)OSX};
+    const uint64_t img_str[3] = {(uint64_t)Y * OSX * n8, (uint64_t)OSX * n8, n8};
+    const uint64_t grid_dims[4] = {(uint64_t)ncol, (uint64_t)OSY, (uint64_t)OSZ, (uint64_t)OSX};
+    const uint64_t grid_str[3] = {(uint64_t)OSX * n8, (uint64_t)OSY * OSX * n8, n8};
+    const uint32_t img_box[4] = {(uint32_t)kYzCW, (uint32_t)ZR, (uint32_t)(adj ? Y / 2 : OSY / 2), 1};
+    const uint32_t grid_box[4] = {(uint32_t)kYzCW, 2, (uint32_t)(OSZ / 2), 1};
+    CUtensorMap timg, tgrid;
+    if (!encode_map_4d(&timg, p->bufA, img_dims, img_str, img_box) ||
+        !encode_map_4d(&tgrid, p->bufA, grid_dims, grid_str, grid_box))
+        return TR_OK;
+    const size_t smem = yz_smem_bytes(OSY, OSZ, ZR);
+    TR_TRY(set_smem_limit(fn, smem));
+    if (CL > 8) TR_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((int64_t)OSX * (ncol / kYzCW) * CL));
+    cfg.blockDim = dim3((unsigned)kYzNT);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg) != cudaSuccess || clusters < 1) {
+        cudaGetLastError();                 // the device cannot hold such a cluster: separate passes
+        return TR_OK;
+    }
+    YzArgs ya;
+    ya.Z = Z;
+    ya.Y = Y;
+    ya.pad_z = p->ax[0].pad;
+    ya.pad_y = p->ax[1].pad;
+    ya.ncol = ncol;
+    ya.twz = p->ax[0].twiddle;
+    ya.twy = p->ax[1].twiddle;
+    ya.err = p->dev_err;
+    ya.poll = p->poll_limit;
+    void* args[] = {&ya, adj ? (void*)&tgrid : (void*)&timg, adj ? (void*)&timg : (void*)&tgrid};
+    TR_CUDA(cudaLaunchKernelExC(&cfg, fn, args));
+    *done = true;
+    return TR_OK;
+}
+
 // y pass: [Z][Y -> OSY][OSX * ncol]
 static tr_status stage_fwd_y(tr_plan* p, int ncol, cudaStream_t st) {
     return launch_line(p, 1, p->bufA, p->bufB, p->n[0], (int64_t)p->os[2] * ncol, p->n[1], p->os[1], p->ax[1].pad, 0,
@@ -1777,8 +2083,12 @@ tr_status nufft_forward_cols(tr_plan* p, int bin, const float2* images, int64_t 
     const int ncol = n_img * C;
     TR_TRY(ensure_nufft_buffers(p, (size_t)ncol));
     TR_TRY(stage_fwd_x(p, images, img_stride, n_img, maps, C, st));
-    TR_TRY(stage_fwd_y(p, ncol, st));
-    TR_TRY(stage_fwd_z(p, ncol, st));
+    bool fused = false;
+    TR_TRY(stage_yz(p, ncol, false, st, &fused));
+    if (!fused) {
+        TR_TRY(stage_fwd_y(p, ncol, st));
+        TR_TRY(stage_fwd_z(p, ncol, st));
+    }
     return stage_interp(p, bin, ncol, mode, sigma, y, out, st);
 }
 
@@ -1837,8 +2147,12 @@ tr_status nufft_adjoint_cols(tr_plan* p, int bin, const float2* ksp, int n_img, 
     TR_TRY(ensure_nufft_buffers(p, (size_t)ncol));
     TR_TRY(tune_spread_cols(p, bin, ksp, ncol, use_dcf, st));
     TR_TRY(stage_spread(p, bin, ksp, ncol, use_dcf, st));
-    TR_TRY(stage_adj_z(p, ncol, st));
-    TR_TRY(stage_adj_y(p, ncol, st));
+    bool fused = false;
+    TR_TRY(stage_yz(p, ncol, true, st, &fused));
+    if (!fused) {
+        TR_TRY(stage_adj_z(p, ncol, st));
+        TR_TRY(stage_adj_y(p, ncol, st));
+    }
     return stage_adj_x(p, n_img, maps, C, images, img_stride, st);
 }
 
@@ -1870,11 +2184,15 @@ tr_status profile_nufft(tr_plan* p, int bin, int reps, double* ms, double* bytes
     bytes[5] = c8 * ncol * (G + YP);
     bytes[6] = c8 * ncol * (YP + XP);
     bytes[7] = c8 * (XP * ncol + C * N + E * N);
+    bytes[8] = c8 * ncol * (XP + G);      // fused forward y + z
+    bytes[9] = c8 * ncol * (G + XP);      // fused adjoint z + y
+    ms[8] = ms[9] = 0.0;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     tr_status rs = TR_OK;
-    for (int s = 0; s < 8 && rs == TR_OK; ++s) {
+    for (int s = 0; s < 10 && rs == TR_OK; ++s) {
+        bool fused = true;
         auto run = [&]() -> tr_status {
             switch (s) {
                 case 0: return stage_fwd_x(p, img, N, E, p->maps, C, st);
@@ -1884,10 +2202,16 @@ tr_status profile_nufft(tr_plan* p, int bin, int reps, double* ms, double* bytes
                 case 4: return stage_spread(p, bin, ksp, ncol, true, st);
                 case 5: return stage_adj_z(p, ncol, st);
                 case 6: return stage_adj_y(p, ncol, st);
-                default: return stage_adj_x(p, E, p->maps, C, img, N, st);
+                case 7: return stage_adj_x(p, E, p->maps, C, img, N, st);
+                case 8: return stage_yz(p, ncol, false, st, &fused);
+                default: return stage_yz(p, ncol, true, st, &fused);
             }
         };
         rs = run();  // warm-up
+        if (rs == TR_OK && !fused) {     // the plan runs these as the separate passes
+            bytes[s] = 0.0;
+            continue;
+        }
         if (rs != TR_OK) break;
         cudaEventRecord(e0, st);
         for (int r = 0; r < reps && rs == TR_OK; ++r) rs = run();
@@ -2259,6 +2583,7 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
     TR_CUDA(cudaMemset(p->dev_err, 0, sizeof(int)));
     *p->err_host = 0;
     p->use_tma = (d->flags & TR_PLAN_NO_TMA) == 0;
+    p->fuse_yz = (d->flags & TR_PLAN_YZ_FUSION) != 0;
     p->autotune = (d->flags & TR_PLAN_AUTOTUNE) != 0;
     p->workspace_bytes = (int64_t)(nks * (sizeof(float4) + sizeof(TapRec) + sizeof(int32_t)) +
                                    glist.size() * sizeof(int2) + (gwork.size() + gsplits.size()) * sizeof(int4) +

@@ -25,6 +25,15 @@
 
 namespace tr {
 
+// Text of the device error word's bits (kDevErr*).
+static std::string device_error_text(int bits) {
+    std::string s;
+    if (bits & kDevErrTmaWait) s += "a bounded device wait expired";
+    if (bits & kDevErrCluster) s += std::string(s.empty() ? "" : " and ") + "a cluster kernel ran without its cluster";
+    if (s.empty()) s = "a device-side check failed";
+    return s + " (error bits " + std::to_string(bits) + ")";
+}
+
 struct PdhgGraph {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -502,8 +511,8 @@ static tr_status run_impl(tr_plan* p, const tr_pdhg_state* s, const tr_pdhg_para
             *p->err_host = 0;
             cudaMemsetAsync(p->dev_err, 0, sizeof(int), st);
             if (done) *done = it;
-            return fail(TR_ERR_TIMEOUT, "a bounded device wait expired in iteration " + std::to_string(it) +
-                                            " (error bits " + std::to_string(bits) + "); results are invalid");
+            return fail(TR_ERR_TIMEOUT, device_error_text(bits) + " in iteration " + std::to_string(it) +
+                                            "; results are invalid");
         }
         const double t = tolerance_from(q, p->tol_host[0], p->tol_host[1]);
         if (hist) hist[it] = t;
@@ -557,8 +566,7 @@ extern "C" tr_status tr_pdhg_phase(tr_plan* plan, const tr_pdhg_state* state, co
         const int bits = *plan->err_host;
         *plan->err_host = 0;
         cudaMemsetAsync(plan->dev_err, 0, sizeof(int), (cudaStream_t)stream);
-        return fail(TR_ERR_TIMEOUT, "a bounded device wait expired in an earlier phase (error bits " +
-                                        std::to_string(bits) + "); results are invalid");
+        return fail(TR_ERR_TIMEOUT, device_error_text(bits) + " in an earlier phase; results are invalid");
     }
     int prev = -1;
     cudaGetDevice(&prev);

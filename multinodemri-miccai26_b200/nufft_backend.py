@@ -118,7 +118,7 @@ class B200NufftBackend(NufftBackend):
     """
 
     def __init__(self, img_shape, coordinates, device=0, *, dcf: Iterable | None = None, n_coils: int = 1,
-                 n_echoes: int = 1, autotune: bool = False, tma: bool = True) -> None:
+                 n_echoes: int = 1, autotune: bool = False, tma: bool = True, fuse_yz: bool = False) -> None:
         super().__init__(img_shape)
         import torch
         self._torch = torch
@@ -159,7 +159,8 @@ class B200NufftBackend(NufftBackend):
         desc.oversamp = 1.25
         desc.width = 4
         desc.device = self.device_index
-        desc.flags = (_lib.TR_PLAN_AUTOTUNE if autotune else 0) | (0 if tma else _lib.TR_PLAN_NO_TMA)
+        desc.flags = ((_lib.TR_PLAN_AUTOTUNE if autotune else 0) | (0 if tma else _lib.TR_PLAN_NO_TMA)
+                      | (_lib.TR_PLAN_YZ_FUSION if fuse_yz else 0))
         handle = ctypes.c_void_p()
         _lib.check(lib.tr_plan_create(ctypes.byref(desc), ctypes.byref(handle)), "tr_plan_create")
         self._plan = handle
@@ -341,17 +342,27 @@ class B200NufftBackend(NufftBackend):
         once, the next PDHG call then raises with TR_ERR_TIMEOUT)."""
         _lib.check(self._lib.tr_plan_set_wait_limit(self._plan, int(polls)), "tr_plan_set_wait_limit")
 
-    STAGES = ("fwd_x", "fwd_y", "fwd_z", "interp", "spread", "adj_z", "adj_y", "adj_x")
+    STAGES = ("fwd_x", "fwd_y", "fwd_z", "interp", "spread", "adj_z", "adj_y", "adj_x", "fwd_yz", "adj_zy")
+    # the stages one batched forward + adjoint runs, with and without the fused y / z passes
+    PIPELINE_FUSED = ("fwd_x", "fwd_yz", "interp", "spread", "adj_zy", "adj_x")
+    PIPELINE_SEPARATE = ("fwd_x", "fwd_y", "fwd_z", "interp", "spread", "adj_z", "adj_y", "adj_x")
 
     def profile(self, bin_index: int = 0, reps: int = 5) -> dict:
-        """CUDA-event time (ms) and algorithmic bytes of each NUFFT stage of one bin."""
+        """CUDA-event time (ms) and algorithmic bytes of each NUFFT stage of one
+        bin; ``fwd_yz`` / ``adj_zy`` (the fused y + z passes) are absent when the
+        plan runs the separate passes.  ``pipeline(profile)`` lists the stages
+        the solver actually runs."""
         b = self._validate_bin(bin_index)
-        ms = (ctypes.c_double * 8)()
-        by = (ctypes.c_double * 8)()
+        ms = (ctypes.c_double * 10)()
+        by = (ctypes.c_double * 10)()
         _lib.check(self._lib.tr_profile_nufft(self._plan, b, int(reps), ms, by, self._stream()), "profile")
         self._torch.cuda.synchronize(self.device)
         return {name: {"ms": ms[i], "bytes": by[i], "gbs": by[i] / (ms[i] * 1e6) if ms[i] > 0 else 0.0}
-                for i, name in enumerate(self.STAGES)}
+                for i, name in enumerate(self.STAGES) if i < 8 or ms[i] > 0}
+
+    @classmethod
+    def pipeline(cls, prof: dict) -> tuple:
+        return cls.PIPELINE_FUSED if "fwd_yz" in prof and "adj_zy" in prof else cls.PIPELINE_SEPARATE
 
     @property
     def spread_columns(self) -> int:

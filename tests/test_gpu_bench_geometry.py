@@ -81,3 +81,34 @@ def test_adjoint_96_columns_matches_oracle(problem):
     # the gather is deterministic at this size too
     g2 = be.adjoint_bin(qs, 0, use_dcf=True)
     assert torch.equal(g2, be.adjoint_bin(qs, 0, use_dcf=True))
+
+
+@pytest.mark.parametrize("shape,E,C", [(SHAPE, E, C), ((96, 128, 128), 4, 8)])
+def test_fused_yz_passes_equal_the_separate_passes(shape, E, C):
+    """The fused y + z kernels (one thread-block cluster per (x, 4-column) plane,
+    the intermediate volume in distributed shared memory) run each line through
+    the same butterflies as the separate passes: the NUFFT results are equal
+    bit for bit.  Shapes: the benchmark's (16-CTA clusters) and the 128x128x96
+    TVME workload's (8-CTA clusters).  Plans use them only when asked
+    (fuse_yz=True, TR_PLAN_YZ_FUSION): they measured slower than the separate
+    passes."""
+    torch = _torch()
+    syn = pkg("synthetic")
+    nb = pkg("nufft_backend")
+    rng = np.random.default_rng(11)
+    k = syn.cones_trajectory(shape, 512, 300, rng)[:48].reshape(-1, 3)
+    dcf = syn.density(k, shape)
+    mps = syn.coil_maps(shape, C, rng)
+    img = torch.randn((E,) + shape, dtype=torch.complex64, device="cuda")
+    q = torch.randn((k.shape[0], E * C), dtype=torch.complex64, device="cuda")
+    outs = []
+    for fuse in (True, False):
+        be = nb.B200NufftBackend(shape, [k], 0, dcf=[dcf], n_coils=C, n_echoes=E, fuse_yz=fuse)
+        be.set_maps(mps)
+        prof = be.profile(0, reps=1)
+        assert ("fwd_yz" in prof and "adj_zy" in prof) == fuse      # the fused kernels ran when allowed
+        outs.append((be.forward_bin(img, 0).clone(), be.adjoint_bin(q, 0, use_dcf=True).clone()))
+        be.close()
+    torch.cuda.synchronize()
+    assert torch.equal(outs[0][0], outs[1][0])
+    assert torch.equal(outs[0][1], outs[1][1])
