@@ -38,6 +38,7 @@ def main(argv=None):
     ap.add_argument("--pdhg", type=int, default=0, help="also run this many TVME iterations (all bins)")
     ap.add_argument("--bins", type=int, default=2)
     ap.add_argument("--no-tma", action="store_true", help="stage the FFT passes with cp.async instead of TMA")
+    ap.add_argument("--fuse-yz", action="store_true", help="also time the fused y + z cluster kernels")
     ap.add_argument("--autotune", action="store_true", help="let the plan time its launch-shape candidates")
     args = ap.parse_args(argv)
     import torch
@@ -48,7 +49,7 @@ def main(argv=None):
     coord = syn.cones_trajectory(shape, args.cones, args.readout, rng).reshape(-1, 3)
     dcf = syn.density(coord, shape)
     be = nb.B200NufftBackend(shape, [coord], 0, dcf=[dcf], n_coils=args.coils, n_echoes=args.echoes,
-                             tma=not args.no_tma, autotune=args.autotune)
+                             tma=not args.no_tma, autotune=args.autotune, fuse_yz=args.fuse_yz)
     mps = syn.coil_maps(shape, args.coils, rng)
     be.set_maps(mps)
     prof = be.profile(0, reps=args.reps)
