@@ -4,8 +4,8 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--config tvme-256] [--impl b200|reference]
 
 Workload (default ``tvme-256``): TVME at 256 x 256 x 128, 16 coils, 6 echoes,
-6 motion bins, 4096 cones x 800 readout points, lambda 1e-5, tol 1e-3, max 300
-iterations, seeded synthetic phantom (the reference's liver dataset is not
+6 motion bins, 4096 cones x 800 readout points, lambda 1e-5, tol 1e-3, max 1000
+iterations (a cap the solve does not reach), seeded synthetic phantom (the reference's liver dataset is not
 available).  A "step" is one PDHG iteration over the whole batch (every bin,
 echo and coil).  W warm-up steps, then K steps timed with CUDA events on the
 solver's stream; then a full plain (zero-start) solve to tolerance and, when a
