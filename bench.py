@@ -74,10 +74,13 @@ NCU_TRAFFIC_16COL = {
     "spread": 2.296e9, "adj_z": 3.732e9, "adj_y": 2.984e9, "adj_x": 2.012e9,
 }
 
-# Iterations to --tol of plain PDHG on each seeded workload, measured with the
-# b200 arm on the same seeded problem; the CPU reference arm cannot run a full
-# solve within minutes and extrapolates its per-iteration time with these.
-ITERS_TO_TOL = {"tvme-256": None, "tvme-256-dirichlet": None, "tvme-128": None, "tvmw-160": None, "tvm-64": 100}
+# Iterations to --tol of plain PDHG with the reference's steps (sigma = tau =
+# 1/6) on each seeded workload, measured with the b200 arm on the same seeded
+# problem (TVME-256: `bench.py --step-rule reference --max-iter 2000`, tol
+# 0.000999 at iteration 510); None: the configuration's max_iter (the rule is not
+# met before it).  The CPU reference arm cannot run a full solve within minutes
+# and extrapolates its per-iteration time with these.
+ITERS_TO_TOL = {"tvme-256": 510, "tvme-256-dirichlet": None, "tvme-128": None, "tvmw-160": None, "tvm-64": 100}
 
 
 def parse(argv=None):

@@ -159,16 +159,21 @@ __device__ __forceinline__ void cluster_sync_all() {
 }
 
 // -i * z
-__device__ __forceinline__ float2 mul_mi(float2 z) { return make_float2(z.y, -z.x); }
+__host__ __device__ __forceinline__ float2 mul_mi(float2 z) { return make_float2(z.y, -z.x); }
 // +i * z
-__device__ __forceinline__ float2 mul_pi(float2 z) { return make_float2(-z.y, z.x); }
+__host__ __device__ __forceinline__ float2 mul_pi(float2 z) { return make_float2(-z.y, z.x); }
+// z * exp(-i theta) (forward) or z * exp(+i theta) (inverse), with c = cos theta, s = sin theta
+__host__ __device__ __forceinline__ float2 crot(float2 z, float c, float s, bool inv) {
+    return inv ? make_float2(fmaf(z.x, c, -z.y * s), fmaf(z.y, c, z.x * s))
+               : make_float2(fmaf(z.x, c, z.y * s), fmaf(z.y, c, -z.x * s));
+}
 
 template <int R>
 struct Dft;
 
 template <>
 struct Dft<2> {
-    __device__ __forceinline__ static void run(float2 (&v)[2], bool) {
+    __host__ __device__ __forceinline__ static void run(float2 (&v)[2], bool) {
         float2 a = v[0], b = v[1];
         v[0] = cadd_p(a, b);
         v[1] = csub_p(a, b);
@@ -177,7 +182,7 @@ struct Dft<2> {
 
 template <>
 struct Dft<4> {
-    __device__ __forceinline__ static void run(float2 (&v)[4], bool inv) {
+    __host__ __device__ __forceinline__ static void run(float2 (&v)[4], bool inv) {
         float2 s0 = cadd_p(v[0], v[2]), d0 = csub_p(v[0], v[2]);
         float2 s1 = cadd_p(v[1], v[3]), d1 = csub_p(v[1], v[3]);
         float2 rd1 = inv ? mul_pi(d1) : mul_mi(d1);
@@ -190,7 +195,7 @@ struct Dft<4> {
 
 template <>
 struct Dft<8> {
-    __device__ __forceinline__ static void run(float2 (&v)[8], bool inv) {
+    __host__ __device__ __forceinline__ static void run(float2 (&v)[8], bool inv) {
         const float h = 0.70710678118654752f;
         float2 a[4], b[4];
 #pragma unroll
@@ -226,31 +231,31 @@ template <int R>
 struct OddTables;
 template <>
 struct OddTables<3> {
-    __device__ __forceinline__ static float c(int k) { return -0.5f; }
-    __device__ __forceinline__ static float s(int k) { return 0.86602540378443865f; }
+    __host__ __device__ __forceinline__ static float c(int k) { return -0.5f; }
+    __host__ __device__ __forceinline__ static float s(int k) { return 0.86602540378443865f; }
 };
 template <>
 struct OddTables<5> {
-    __device__ __forceinline__ static float c(int k) {
+    __host__ __device__ __forceinline__ static float c(int k) {
         return k == 1 ? 0.30901699437494742f : -0.80901699437494742f;
     }
-    __device__ __forceinline__ static float s(int k) {
+    __host__ __device__ __forceinline__ static float s(int k) {
         return k == 1 ? 0.95105651629515357f : 0.58778525229247313f;
     }
 };
 template <>
 struct OddTables<7> {
-    __device__ __forceinline__ static float c(int k) {
+    __host__ __device__ __forceinline__ static float c(int k) {
         return k == 1 ? 0.62348980185873353f : (k == 2 ? -0.22252093395631440f : -0.90096886790241913f);
     }
-    __device__ __forceinline__ static float s(int k) {
+    __host__ __device__ __forceinline__ static float s(int k) {
         return k == 1 ? 0.78183148246802981f : (k == 2 ? 0.97492791218182361f : 0.43388373911755812f);
     }
 };
 
 template <int R>
 struct DftOdd {
-    __device__ __forceinline__ static void run(float2 (&v)[R], bool inv) {
+    __host__ __device__ __forceinline__ static void run(float2 (&v)[R], bool inv) {
         constexpr int H = (R - 1) / 2;
         float2 s[H + 1], d[H + 1];
 #pragma unroll
@@ -290,6 +295,76 @@ template <>
 struct Dft<5> : DftOdd<5> {};
 template <>
 struct Dft<7> : DftOdd<7> {};
+
+// Composite radices for two-pass transforms (fewer shared-memory round trips).
+// 16 = 4 x 4 (Cooley-Tukey): n = 4 n1 + n2, k = k1 + 4 k2,
+//   X[k1 + 4 k2] = sum_n2 W16^(n2 k1) W4^(n2 k2) sum_n1 x[4 n1 + n2] W4^(n1 k1).
+template <>
+struct Dft<16> {
+    __host__ __device__ __forceinline__ static void run(float2 (&v)[16], bool inv) {
+        const float c1 = 0.92387953251128674f, s1 = 0.38268343236508978f, h = 0.70710678118654752f;
+        float2 a[4][4];
+#pragma unroll
+        for (int n2 = 0; n2 < 4; ++n2) {
+            float2 t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+            Dft<4>::run(t, inv);
+#pragma unroll
+            for (int k1 = 0; k1 < 4; ++k1) a[n2][k1] = t[k1];
+        }
+        // twiddles W16^m, m = n2 k1 in {1, 2, 3, 4, 6, 9}
+        a[1][1] = crot(a[1][1], c1, s1, inv);
+        a[1][2] = crot(a[1][2], h, h, inv);
+        a[1][3] = crot(a[1][3], s1, c1, inv);
+        a[2][1] = crot(a[2][1], h, h, inv);
+        a[2][2] = inv ? mul_pi(a[2][2]) : mul_mi(a[2][2]);
+        a[2][3] = crot(a[2][3], -h, h, inv);
+        a[3][1] = crot(a[3][1], s1, c1, inv);
+        a[3][2] = crot(a[3][2], -h, h, inv);
+        a[3][3] = crot(a[3][3], -c1, -s1, inv);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) {
+            float2 t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+            Dft<4>::run(t, inv);
+#pragma unroll
+            for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = t[k2];
+        }
+    }
+};
+
+// Coprime N1 x N2 (Good-Thomas prime-factor algorithm, no twiddles):
+//   n = (N2 n1 + N1 n2) mod N,  k = (N2 t1 k1 + N1 t2 k2) mod N,
+// t1 = N2^-1 mod N1, t2 = N1^-1 mod N2; then W_N^(n k) = W_N1^(n1 k1) W_N2^(n2 k2).
+template <int N1, int N2, int T1, int T2>
+struct DftPfa {
+    __host__ __device__ __forceinline__ static void run(float2 (&v)[N1 * N2], bool inv) {
+        constexpr int N = N1 * N2;
+        float2 b[N2][N1];
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) {
+            float2 t[N1];
+#pragma unroll
+            for (int n1 = 0; n1 < N1; ++n1) t[n1] = v[(N2 * n1 + N1 * n2) % N];
+            Dft<N1>::run(t, inv);
+#pragma unroll
+            for (int k1 = 0; k1 < N1; ++k1) b[n2][k1] = t[k1];
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) {
+            float2 t[N2];
+#pragma unroll
+            for (int n2 = 0; n2 < N2; ++n2) t[n2] = b[n2][k1];
+            Dft<N2>::run(t, inv);
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2) v[(N2 * T1 * k1 + N1 * T2 * k2) % N] = t[k2];
+        }
+    }
+};
+// 10 = 2 x 5: t1 = 5^-1 mod 2 = 1, t2 = 2^-1 mod 5 = 3
+template <>
+struct Dft<10> : DftPfa<2, 5, 1, 3> {};
+// 20 = 4 x 5: t1 = 5^-1 mod 4 = 1, t2 = 4^-1 mod 5 = 4
+template <>
+struct Dft<20> : DftPfa<4, 5, 1, 4> {};
 
 // One Stockham stage over every butterfly of every column.
 template <int R, class Src, class Dst>
@@ -361,18 +436,50 @@ __host__ __device__ constexpr int ct_nstages(int L) {
     while (ct_radix(L, s) != 0) ++s;
     return s;
 }
+// Radix plans.  P = 0: the sequence above (L = 320 -> 5, 8, 8: three passes
+// through shared memory).  P = 1: two passes where a composite radix exists
+// (320 = 20 x 16, 160 = 10 x 16): each pass moves every element through
+// shared memory once each way, and the transforms that are bound by the
+// shared-memory data pipe lose a third of that traffic; other lengths keep P = 0.
+__host__ __device__ constexpr int ct_radix_p(int P, int L, int s) {
+    if (P == 1 && L == 320) return s == 0 ? 20 : (s == 1 ? 16 : 0);
+    if (P == 1 && L == 160) return s == 0 ? 10 : (s == 1 ? 16 : 0);
+    return ct_radix(L, s);
+}
+__host__ __device__ constexpr int ct_nstages_p(int P, int L) {
+    int s = 0;
+    while (ct_radix_p(P, L, s) != 0) ++s;
+    return s;
+}
+// Row swizzle of a two-pass plan's intermediate tile.  With 64-byte rows (8
+// columns) and an even first radix R0, the rows R0 j + r that the butterflies
+// j and j + 1 of a half-warp write lie in the same half of the 32 banks (a
+// 2-way conflict on every store); exchanging rows 2i and 2i + 1 within every
+// odd block of R0 rows puts them in opposite halves, and the second pass reads
+// its rows j + R0 r (four consecutive rows per warp) through the same map.
+// Returns R0 where that applies, else 0 (no swizzle).
+__host__ __device__ constexpr int ct_swz_p(int P, int L, int row_elems) {
+    return (P == 1 && ct_nstages_p(P, L) == 2 && ct_radix_p(P, L, 0) % 2 == 0 && row_elems == 8)
+               ? ct_radix_p(P, L, 0) : 0;
+}
+template <int SW>
+__device__ __forceinline__ int ct_swz_row(int m) {
+    if constexpr (SW == 0) return m;
+    else return m ^ ((m / SW) & 1);
+}
 
-template <int L, int W, int NT, bool INV, int s, int Ns, bool LD = false>
+template <int L, int W, int NT, bool INV, int s, int Ns, bool LD = false, int P = 0>
 struct CtStage {
     template <class Load, class Store>
     __device__ __forceinline__ static void run(const float2* __restrict__ src, float2* __restrict__ dst,
                                                const float2* __restrict__ tw, Load& load, Store& store) {
-        constexpr int S = ct_nstages(L);
-        constexpr int R = ct_radix(L, s);
+        constexpr int S = ct_nstages_p(P, L);
+        constexpr int R = ct_radix_p(P, L, s);
         constexpr int NB = L / R;
         constexpr int TOTAL = NB * W;
         constexpr int STEP = L / (Ns * R);
         constexpr int ITERS = (TOTAL + NT - 1) / NT;
+        constexpr int SW = ct_swz_p(P, L, W);          // stage 0 writes / stage 1 reads swizzled rows
 #pragma unroll
         for (int it = 0; it < ITERS; ++it) {
             const int idx = (int)threadIdx.x + it * NT;
@@ -385,7 +492,7 @@ struct CtStage {
                 for (int r = 0; r < R; ++r) {
                     float2 x;
                     if constexpr (LD && s == 0) x = load(j + r * NB, w);
-                    else x = src[(j + r * NB) * W + w];
+                    else x = src[ct_swz_row<(s == 1 ? SW : 0)>(j + r * NB) * W + w];
                     if (Ns > 1 && r > 0) {
                         float2 t = tw[k * r * STEP];
                         if (INV) t.y = -t.y;
@@ -398,13 +505,13 @@ struct CtStage {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     if (s == S - 1) store(d0 + r * Ns, w, v[r]);
-                    else dst[(d0 + r * Ns) * W + w] = v[r];
+                    else dst[ct_swz_row<(s == 0 ? SW : 0)>(d0 + r * Ns) * W + w] = v[r];
                 }
             }
         }
         if constexpr (s < S - 1) {
             __syncthreads();
-            CtStage<L, W, NT, INV, s + 1, Ns * R, LD>::run(dst, const_cast<float2*>(src), tw, load, store);
+            CtStage<L, W, NT, INV, s + 1, Ns * R, LD, P>::run(dst, const_cast<float2*>(src), tw, load, store);
         }
     }
 };
@@ -414,10 +521,15 @@ struct CtStage {
 struct NoLoad {
     __device__ __forceinline__ float2 operator()(int, int) const { return make_float2(0.f, 0.f); }
 };
-template <int L, int W, int NT, bool INV, class Store>
+template <int L, int W, int NT, bool INV, class Store, int P = 0>
 __device__ __forceinline__ void fft_ct(float2* A, float2* B, const float2* tw, Store& store) {
     NoLoad none;
-    CtStage<L, W, NT, INV, 0, 1>::run(A, B, tw, none, store);
+    CtStage<L, W, NT, INV, 0, 1, false, P>::run(A, B, tw, none, store);
+}
+template <int P, int L, int W, int NT, bool INV, class Store>
+__device__ __forceinline__ void fft_ct_p(float2* A, float2* B, const float2* tw, Store& store) {
+    NoLoad none;
+    CtStage<L, W, NT, INV, 0, 1, false, P>::run(A, B, tw, none, store);
 }
 
 // Same transform with the first stage reading its inputs from load(m, w)
@@ -427,6 +539,10 @@ template <int L, int W, int NT, bool INV, class Load, class Store>
 __device__ __forceinline__ void fft_ct_ld(float2* A, float2* B, const float2* tw, Load& load, Store& store) {
     CtStage<L, W, NT, INV, 0, 1, true>::run(A, B, tw, load, store);
 }
+template <int P, int L, int W, int NT, bool INV, class Load, class Store>
+__device__ __forceinline__ void fft_ct_ld_p(float2* A, float2* B, const float2* tw, Load& load, Store& store) {
+    CtStage<L, W, NT, INV, 0, 1, true, P>::run(A, B, tw, load, store);
+}
 
 // In-place variant: every stage first reads all of a thread's butterflies into
 // registers, the CTA synchronises, and the results go back into the same
@@ -435,16 +551,17 @@ __device__ __forceinline__ void fft_ct_ld(float2* A, float2* B, const float2* tw
 // fft_ct (bit-identical results) with half the shared memory.
 // RS: row stride of the buffer in elements (the W transformed columns are the
 // first W of each row; RS > W transforms a column subset of a wider tile).
-template <int L, int W, int NT, bool INV, int s, int Ns, int RS = W>
+template <int L, int W, int NT, bool INV, int s, int Ns, int RS = W, int P = 0>
 struct CtStageIP {
     template <class Store>
     __device__ __forceinline__ static void run(float2* buf, const float2* __restrict__ tw, Store& store) {
-        constexpr int S = ct_nstages(L);
-        constexpr int R = ct_radix(L, s);
+        constexpr int S = ct_nstages_p(P, L);
+        constexpr int R = ct_radix_p(P, L, s);
         constexpr int NB = L / R;
         constexpr int TOTAL = NB * W;
         constexpr int STEP = L / (Ns * R);
         constexpr int ITERS = (TOTAL + NT - 1) / NT;
+        constexpr int SW = ct_swz_p(P, L, RS);
         float2 v[ITERS][R];
 #pragma unroll
         for (int it = 0; it < ITERS; ++it) {
@@ -455,7 +572,7 @@ struct CtStageIP {
                 const int k = (Ns == 1) ? 0 : j % Ns;
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    float2 x = buf[(j + r * NB) * RS + w];
+                    float2 x = buf[ct_swz_row<(s == 1 ? SW : 0)>(j + r * NB) * RS + w];
                     if (Ns > 1 && r > 0) {
                         float2 t = tw[k * r * STEP];
                         if (INV) t.y = -t.y;
@@ -478,19 +595,23 @@ struct CtStageIP {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     if (s == S - 1) store(d0 + r * Ns, w, v[it][r]);
-                    else buf[(d0 + r * Ns) * RS + w] = v[it][r];
+                    else buf[ct_swz_row<(s == 0 ? SW : 0)>(d0 + r * Ns) * RS + w] = v[it][r];
                 }
             }
         }
         if constexpr (s < S - 1) {
             __syncthreads();
-            CtStageIP<L, W, NT, INV, s + 1, Ns * R, RS>::run(buf, tw, store);
+            CtStageIP<L, W, NT, INV, s + 1, Ns * R, RS, P>::run(buf, tw, store);
         }
     }
 };
 template <int L, int W, int NT, bool INV, class Store>
 __device__ __forceinline__ void fft_ct_ip(float2* buf, const float2* tw, Store& store) {
     CtStageIP<L, W, NT, INV, 0, 1>::run(buf, tw, store);
+}
+template <int P, int L, int W, int NT, bool INV, class Store>
+__device__ __forceinline__ void fft_ct_ip_p(float2* buf, const float2* tw, Store& store) {
+    CtStageIP<L, W, NT, INV, 0, 1, W, P>::run(buf, tw, store);
 }
 // The same on the first W columns of an [L][RS] buffer.
 template <int L, int W, int RS, int NT, bool INV, class Store>
@@ -499,9 +620,9 @@ __device__ __forceinline__ void fft_ct_ip_rs(float2* buf, const float2* tw, Stor
 }
 
 // Buffer that the last stage of an L-point fft_ct does not read.
-template <int L>
+template <int L, int P = 0>
 __device__ __forceinline__ float2* fft_ct_free(float2* A, float2* B) {
-    return ((ct_nstages(L) - 1) % 2 == 0) ? B : A;
+    return ((ct_nstages_p(P, L) - 1) % 2 == 0) ? B : A;
 }
 
 // Full transform: load(m, w) -> input element m of column w; store(k, w, v)

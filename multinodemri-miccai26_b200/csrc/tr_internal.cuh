@@ -78,7 +78,7 @@ __device__ __forceinline__ float2 f2_unpack(unsigned long long r) {
 }
 #endif
 // a + b
-__device__ __forceinline__ float2 cadd_p(float2 a, float2 b) {
+__host__ __device__ __forceinline__ float2 cadd_p(float2 a, float2 b) {
 #if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
     unsigned long long r;
     asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_pack(a)), "l"(f2_pack(b)));
@@ -88,7 +88,7 @@ __device__ __forceinline__ float2 cadd_p(float2 a, float2 b) {
 #endif
 }
 // a - b
-__device__ __forceinline__ float2 csub_p(float2 a, float2 b) {
+__host__ __device__ __forceinline__ float2 csub_p(float2 a, float2 b) {
 #if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
     unsigned long long r;
     asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_pack(a)), "l"(f2_pack(b)));
@@ -98,7 +98,7 @@ __device__ __forceinline__ float2 csub_p(float2 a, float2 b) {
 #endif
 }
 // c + w * v (real w on both components)
-__device__ __forceinline__ float2 cfma_real(float w, float2 v, float2 c) {
+__host__ __device__ __forceinline__ float2 cfma_real(float w, float2 v, float2 c) {
 #if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
     unsigned long long r;
     asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(f2_pack(make_float2(w, w))), "l"(f2_pack(v)), "l"(f2_pack(c)));
@@ -108,7 +108,7 @@ __device__ __forceinline__ float2 cfma_real(float w, float2 v, float2 c) {
 #endif
 }
 // a * b as a.x * (b.x, b.y) + a.y * (-b.y, b.x): one packed multiply, one packed FMA
-__device__ __forceinline__ float2 cmul_p(float2 a, float2 b) {
+__host__ __device__ __forceinline__ float2 cmul_p(float2 a, float2 b) {
 #if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
     unsigned long long t, r;
     asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(t) : "l"(f2_pack(make_float2(a.y, a.y))), "l"(f2_pack(make_float2(-b.y, b.x))));
@@ -220,6 +220,8 @@ struct tr_plan {
     int spread_cols = 128;       // most k-space columns per gridding CTA
     bool use_tma = true;
     bool fuse_yz = false;        // TR_PLAN_YZ_FUSION: fused y + z passes where the geometry allows
+    bool x_two_pass = true;      // 320-point TMA x passes in two shared-memory passes (not TR_PLAN_THREE_PASS_X)
+    bool two_pass_lines[3] = {false, false, false};   // per axis: 160 / 320-point TMA line passes in two passes
     bool autotune = false;       // TR_PLAN_AUTOTUNE: time launch-shape candidates on first use
     std::map<int, int> spread_cols_tuned;   // column count -> chosen spread_cols         // TMA-tiled FFT passes where the geometry allows
     // TVMW

@@ -373,6 +373,17 @@ __host__ __device__ constexpr int line_threads(int L, int W) {
     return ct_rounds(L, W, 320) < ct_rounds(L, W, 256) ? 320 : 256;
 }
 static size_t line_tma_smem_bytes(int L, int W) { return (size_t)(L * W + L) * sizeof(float2) + 128; }
+// Threads and CTAs per SM of a line pass with radix plan P (P = 1: two passes,
+// one round each: as many threads as the larger pass has butterflies;
+// 320 x 8: 128 and 160 -> 160; 160 x 16: 256 and 160 -> 256).
+__host__ __device__ constexpr int line_threads_p(int L, int W, int P) {
+    return P == 0 ? line_threads(L, W)
+                  : ((L / ct_radix_p(P, L, 0)) * W > (L / ct_radix_p(P, L, 1)) * W ? (L / ct_radix_p(P, L, 0)) * W
+                                                                                    : (L / ct_radix_p(P, L, 1)) * W);
+}
+__host__ __device__ constexpr int line_min_ctas(int NT, int P) {
+    return P == 0 ? (NT == 320 ? 5 : 6) : (NT <= 160 ? 6 : 4);
+}
 
 template <int L, int W, bool INV>
 __global__ void __launch_bounds__(256) k_line_ct(LineArgs a) {
@@ -441,8 +452,8 @@ __global__ void __launch_bounds__(256) k_line_ct(LineArgs a) {
 // One thread issues every copy; the rest of the CTA only runs the transform.
 // The load wait is bounded: on expiry the CTA waits (bounded) for its copies
 // in flight, sets kDevErrTmaWait and exits.
-template <int L, int W, bool INV, int NT = line_threads(L, W)>
-__global__ void __launch_bounds__(NT, (NT == 320 ? 5 : 6))
+template <int L, int W, bool INV, int P = 0, int NT = line_threads_p(L, W, P)>
+__global__ void __launch_bounds__(NT, line_min_ctas(NT, P))
     k_line_tma(LineArgs a, const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout) {
     extern __shared__ __align__(128) unsigned char tsm_raw[];
     __shared__ __align__(8) uint64_t bar;
@@ -467,7 +478,7 @@ __global__ void __launch_bounds__(NT, (NT == 320 ? 5 : 6))
     }
     float2* ep = smA;
     auto store = [ep](int k, int w, float2 v) { ep[k * W + w] = v; };
-    fft_ct_ip<L, W, NT, INV>(smA, tws, store);
+    fft_ct_ip_p<P, L, W, NT, INV>(smA, tws, store);
     fence_proxy_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1106,6 +1117,169 @@ __global__ void __launch_bounds__(NT, MINB) k_adj_x_tma(AdjXArgs a, const __grid
     }
 }
 
+// ------------------------------------------------------------------ two-pass TMA x passes
+// The same work as k_fwd_x_tma / k_adj_x_tma with the L-point transform in two
+// passes through shared memory (radix plan 1: 320 = 20 x 16) instead of three
+// (5, 8, 8).  The x passes are bound by the shared-memory data pipe (ncu on
+// k_adj_x_tma: LSU wavefronts at 88 % of peak, DRAM at 40 %), and a pass
+// moves every element through shared memory once each way.  kWideNT threads:
+// the radix-16 pass has L/16 x W = 160 butterflies, the radix-20 pass 128.
+constexpr int kWideNT = 160;
+
+template <int L, int W>
+__global__ void __launch_bounds__(kWideNT, 5) k_fwd_x_wide(FwdXArgs a, const __grid_constant__ CUtensorMap timg,
+                                                           const __grid_constant__ CUtensorMap tmap,
+                                                           const __grid_constant__ CUtensorMap tout) {
+    constexpr int NT = kWideNT;
+    extern __shared__ __align__(128) unsigned char xsm_raw[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ float s_apzy;
+    float2* sm = align128(xsm_raw);
+    float2* smA = sm;
+    float2* smB = sm + L * W;
+    float2* tws = sm + 2 * L * W;
+    const int X = a.X;
+    float2* s_img = smA;              // [X]     (the first pass reads these and writes smB)
+    float2* s_map = smA + X;          // [X][W]
+    const int img = (int)(blockIdx.x % (unsigned)a.n_img);
+    const int row = (int)(blockIdx.x / (unsigned)a.n_img);
+    const int c0 = (int)blockIdx.z * W;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(&bar, (unsigned)(X * (W + 1) * sizeof(float2)));
+        tma_load_3d(s_img, &timg, &bar, 0, row, img);
+        tma_load_3d(s_map, &tmap, &bar, c0, 0, row);
+        const int z = row / a.Y, y = row - z * a.Y;
+        s_apzy = a.apz[z] * a.apy[y] * a.scale;
+    }
+    for (int i = threadIdx.x; i < L; i += NT) tws[i] = a.tw[i];
+    const bool ok = mbar_wait_or_drain(&bar, 0, a.poll);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
+        return;
+    }
+    const float apzy = s_apzy;
+    const int h = a.h, pad = a.pad;
+    const float* apx = a.apx;
+    auto load = [=](int m, int w) {
+        int j = m + h;
+        if (j >= L) j -= L;
+        const int x = j - pad;
+        float2 v = make_float2(0.f, 0.f);
+        if (x >= 0 && x < X) v = cscale(cmul(s_img[x], s_map[x * W + w]), apzy * apx[x]);
+        return v;
+    };
+    float2* ep = fft_ct_free<L, 1>(smA, smB);        // smA: the staged row is read by the first pass only
+    auto store = [ep](int k, int w, float2 v) { ep[k * W + w] = v; };
+    fft_ct_ld_p<1, L, W, NT, false>(smA, smB, tws, load, store);
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int col = img * a.C + c0;
+        tma_store_3d(&tout, ep + (L / 2) * W, col, 0, row);
+        tma_store_3d(&tout, ep, col, L / 2, row);
+        tma_store_commit_and_drain();
+    }
+}
+
+// Adjoint: the coil groups' tiles alternate between the two buffers, so the
+// next group's tile loads into the buffer the second pass has just read while
+// this group's epilogue reads the cropped rows written over its input tile.
+// Epilogue: lane l of a warp takes image column x = 16 b + l / 2 of block b
+// (blocks dealt to the warps in turn) and coils 4 (l % 2) .. 4 (l % 2) + 3 of
+// the group, so a warp's coil-map loads cover 1 KB in 8 (C = 8) or 16 lines
+// instead of one 64-byte piece per thread in 32; the two lanes of a column add
+// their products with one butterfly shuffle (the same sum in both lanes).
+constexpr int kWideXBlocks = 4;               // ceil(256 / 16 / (kWideNT / 32)): X <= 256
+
+template <int L, int W>
+__global__ void __launch_bounds__(kWideNT, 5) k_adj_x_wide(AdjXArgs a, const __grid_constant__ CUtensorMap tin) {
+    constexpr int NT = kWideNT;
+    constexpr int NW = NT / 32;
+    static_assert(W == 8, "four coils per lane of a 2-lane column group");
+    extern __shared__ __align__(128) unsigned char xsm_raw[];
+    __shared__ __align__(8) uint64_t bar;
+    float2* sm = align128(xsm_raw);
+    float2* tin_buf = sm;                   // this group's input tile; the epilogue rows after pass 1
+    float2* work = sm + L * W;              // pass-1 output; the next group's input tile
+    float2* tws = sm + 2 * L * W;
+    const int X = a.X;
+    // [W][XP] epilogue tile; XP = 2 mod 16 puts the second pass's stores of the
+    // 8 columns of one output row in 8 different 4-bank groups
+    const int XP = X + 2;
+    const int img = (int)(blockIdx.x % (unsigned)a.n_img);
+    const int row = (int)(blockIdx.x / (unsigned)a.n_img);
+    const int lane = (int)threadIdx.x & 31, warp = (int)threadIdx.x >> 5;
+    const int hf = lane & 1;                // coils 4 hf .. 4 hf + 3 of the group
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    for (int i = threadIdx.x; i < L; i += NT) tws[i] = a.tw[i];
+    const int shift = a.h - a.pad;
+    const float4* mrow = reinterpret_cast<const float4*>(a.maps + (int64_t)row * X * a.C);
+    float s[kWideXBlocks];                  // lane 2i: real part of column i's sum; lane 2i + 1: imaginary
+#pragma unroll
+    for (int b = 0; b < kWideXBlocks; ++b) s[b] = 0.f;
+    auto issue = [&](int c0, float2* dst) {
+        mbar_expect_tx(&bar, (unsigned)(L * W * sizeof(float2)));
+        const int col = img * a.C + c0;
+        tma_load_3d(dst, &tin, &bar, col, L / 2, row);
+        tma_load_3d(dst + (L / 2) * W, &tin, &bar, col, 0, row);
+    };
+    __syncthreads();                        // barrier initialised
+    if (threadIdx.x == 0) issue(0, tin_buf);
+    int phase = 0;
+    for (int c0 = 0; c0 < a.C; c0 += W, phase ^= 1) {
+        // one thread polls; the CTA barrier after it is also the barrier between
+        // the previous epilogue's reads and this group's first pass
+        const bool ok = threadIdx.x == 0 ? mbar_wait_or_drain(&bar, (unsigned)phase, a.poll) : true;
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicOr(a.err, kDevErrTmaWait);
+            return;
+        }
+        float2* ep = tin_buf;
+        auto store = [&](int k, int w, float2 v) {
+            int o = k + shift;
+            o = o >= L ? o - L : (o < 0 ? o + L : o);
+            if (o < X) ep[w * XP + o] = v;
+        };
+        fft_ct_p<1, L, W, NT, true>(tin_buf, work, tws, store);
+        __syncthreads();                    // pass 2 done: `work` free, ep complete
+        if (threadIdx.x == 0 && c0 + W < a.C) issue(c0 + W, work);
+        // conj(S) product and the sum over this group's coils
+#pragma unroll
+        for (int b = 0; b < kWideXBlocks; ++b) {
+            const int x = 16 * (warp + NW * b) + (lane >> 1);
+            if (16 * (warp + NW * b) < X) {             // whole blocks: X % 16 == 0
+                const float4* mp = mrow + ((int64_t)x * a.C + c0) / 2 + 2 * hf;
+                const float4 m0 = mp[0], m1 = mp[1];
+                const float2* e = ep + (4 * hf) * XP + x;
+                float2 t = cmulc(e[0], make_float2(m0.x, m0.y));
+                t = cadd(t, cmulc(e[XP], make_float2(m0.z, m0.w)));
+                t = cadd(t, cmulc(e[2 * XP], make_float2(m1.x, m1.y)));
+                t = cadd(t, cmulc(e[3 * XP], make_float2(m1.z, m1.w)));
+                // lane 2i keeps t0.x + t1.x, lane 2i + 1 keeps t0.y + t1.y
+                const float recv = __shfl_xor_sync(0xffffffffu, hf ? t.x : t.y, 1);
+                s[b] += hf ? recv + t.y : t.x + recv;
+            }
+        }
+        float2* t = tin_buf;
+        tin_buf = work;
+        work = t;
+    }
+    const int z = row / a.Y, y = row - z * a.Y;
+    const float szy = a.apz[z] * a.apy[y] * a.scale;
+#pragma unroll
+    for (int b = 0; b < kWideXBlocks; ++b) {
+        const int x = 16 * (warp + NW * b) + (lane >> 1);
+        if (16 * (warp + NW * b) < X) {             // one float per lane: the warp writes 128 contiguous bytes
+            float v = s[b] * (szy * a.apx[x]);
+            float* dst = reinterpret_cast<float*>(a.img + (int64_t)img * a.img_stride + (int64_t)row * X + x) + hf;
+            if (a.accumulate) v = *dst + v;
+            *dst = v;
+        }
+    }
+}
+
 // ------------------------------------------------------------------ per-sample tap records
 // First tap per axis and the 15 KB weights of every (sorted) sample, computed
 // once at plan creation; interpolation and gridding read them instead of
@@ -1667,6 +1841,12 @@ static tr_status launch_line(tr_plan* p, int axis, const float2* in, float2* out
         break;
     switch (A.L) { TR_CT_LENGTHS(TR_LINE_CASE) default: break; }
 #undef TR_LINE_CASE
+    unsigned nt = (unsigned)line_threads(A.L, la.W);
+    if (tma && p->two_pass_lines[axis] && (A.L == 160 || A.L == 320)) {
+        if (A.L == 160) fn = inv ? (const void*)k_line_tma<160, 16, true, 1> : (const void*)k_line_tma<160, 16, false, 1>;
+        else fn = inv ? (const void*)k_line_tma<320, 8, true, 1> : (const void*)k_line_tma<320, 8, false, 1>;
+        nt = (unsigned)line_threads_p(A.L, la.W, 1);
+    }
     if (!fn) fn = (const void*)k_line;
     la.vec16 = ((inner % 2) == 0 && (la.W % 2) == 0 && ((uintptr_t)in % 16) == 0) ? 1 : 0;
     const size_t smem = tma ? line_tma_smem_bytes(A.L, la.W) : fft_smem_bytes(A.L, la.W);
@@ -1674,7 +1854,7 @@ static tr_status launch_line(tr_plan* p, int axis, const float2* in, float2* out
     TR_TRY(set_smem_limit(fn, smem));
     if (tma) {
         void* args[] = {&la, &tin, &tout};
-        TR_CUDA(cudaLaunchKernel(fn, grid, dim3((unsigned)line_threads(A.L, la.W)), args, smem, st));
+        TR_CUDA(cudaLaunchKernel(fn, grid, dim3(nt), args, smem, st));
     } else {
         void* args[] = {&la};
         TR_CUDA(cudaLaunchKernel(fn, grid, dim3(256), args, smem, st));
@@ -1744,15 +1924,20 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
         ok = ok && encode_map_3d(&tout, p->bufA, (uint64_t)fa.ncol, (uint64_t)OSX, nrows, (uint32_t)kTmaXWidth,
                                  (uint32_t)(OSX / 2));
         const void* tfn = nullptr;
+        unsigned nt = 256;
 #define TR_FWDX_TMA(LV) case LV: tfn = (const void*)k_fwd_x_tma<LV, kTmaXWidth>; break;
         switch (OSX) { TR_CT_LENGTHS(TR_FWDX_TMA) default: break; }
 #undef TR_FWDX_TMA
+        if (OSX == 320 && p->x_two_pass) {
+            tfn = (const void*)k_fwd_x_wide<320, kTmaXWidth>;
+            nt = kWideNT;
+        }
         if (ok && tfn) {
             const size_t smem = fft_smem_bytes(OSX, kTmaXWidth) + 128;
             TR_TRY(set_smem_limit(tfn, smem));
             dim3 grid((unsigned)(nrows * n_img), 1u, (unsigned)(C / kTmaXWidth));
             void* args[] = {&fa, &timg, &tmap, &tout};
-            TR_CUDA(cudaLaunchKernel(tfn, grid, dim3(256), args, smem, st));
+            TR_CUDA(cudaLaunchKernel(tfn, grid, dim3(nt), args, smem, st));
             return TR_OK;
         }
     }
@@ -2043,13 +2228,18 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
 #define TR_ADJX_TMA(LV) case LV: tfn = (const void*)k_adj_x_tma<LV, kTmaXWidth>; break;
         switch (OSX) { TR_CT_LENGTHS(TR_ADJX_TMA) default: break; }
 #undef TR_ADJX_TMA
+        unsigned nt = (unsigned)ct_threads(OSX, kTmaXWidth);
+        if (OSX == 320 && p->x_two_pass && X % 16 == 0) {  // X <= 256: kWideXBlocks blocks of 16 per warp
+            tfn = (const void*)k_adj_x_wide<320, kTmaXWidth>;
+            nt = kWideNT;
+        }
         if (tfn && encode_map_3d(&tin, p->bufA, (uint64_t)aa.ncol, (uint64_t)OSX, (uint64_t)Z * Y, (uint32_t)kTmaXWidth,
                                  (uint32_t)(OSX / 2))) {
             const size_t smem = fft_smem_bytes(OSX, kTmaXWidth) + 128;
             TR_TRY(set_smem_limit(tfn, smem));
             dim3 grid((unsigned)((int64_t)Z * Y * n_img));
             void* args[] = {&aa, &tin};
-            TR_CUDA(cudaLaunchKernel(tfn, grid, dim3((unsigned)ct_threads(OSX, kTmaXWidth)), args, smem, st));
+            TR_CUDA(cudaLaunchKernel(tfn, grid, dim3(nt), args, smem, st));
             return TR_OK;
         }
     }
@@ -2584,6 +2774,7 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
     *p->err_host = 0;
     p->use_tma = (d->flags & TR_PLAN_NO_TMA) == 0;
     p->fuse_yz = (d->flags & TR_PLAN_YZ_FUSION) != 0;
+    p->x_two_pass = (d->flags & TR_PLAN_THREE_PASS_X) == 0;
     p->autotune = (d->flags & TR_PLAN_AUTOTUNE) != 0;
     p->workspace_bytes = (int64_t)(nks * (sizeof(float4) + sizeof(TapRec) + sizeof(int32_t)) +
                                    glist.size() * sizeof(int2) + (gwork.size() + gsplits.size()) * sizeof(int4) +

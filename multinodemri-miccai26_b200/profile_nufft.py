@@ -39,6 +39,8 @@ def main(argv=None):
     ap.add_argument("--bins", type=int, default=2)
     ap.add_argument("--no-tma", action="store_true", help="stage the FFT passes with cp.async instead of TMA")
     ap.add_argument("--fuse-yz", action="store_true", help="also time the fused y + z cluster kernels")
+    ap.add_argument("--three-pass-x", action="store_true",
+                    help="run the 320-point x transforms in three shared-memory passes (radices 5, 8, 8)")
     ap.add_argument("--autotune", action="store_true", help="let the plan time its launch-shape candidates")
     args = ap.parse_args(argv)
     import torch
@@ -49,7 +51,8 @@ def main(argv=None):
     coord = syn.cones_trajectory(shape, args.cones, args.readout, rng).reshape(-1, 3)
     dcf = syn.density(coord, shape)
     be = nb.B200NufftBackend(shape, [coord], 0, dcf=[dcf], n_coils=args.coils, n_echoes=args.echoes,
-                             tma=not args.no_tma, autotune=args.autotune, fuse_yz=args.fuse_yz)
+                             tma=not args.no_tma, autotune=args.autotune, fuse_yz=args.fuse_yz,
+                             three_pass_x=args.three_pass_x)
     mps = syn.coil_maps(shape, args.coils, rng)
     be.set_maps(mps)
     prof = be.profile(0, reps=args.reps)

@@ -37,6 +37,14 @@ def ct_radices(L):                    # tr_fft.cuh: ct_radix (7s, 5s, 3s, then 8
     return out
 
 
+def ct_radices_p(P, L):               # tr_fft.cuh: ct_radix_p (P = 1: two passes at 320 and 160)
+    if P == 1 and L == 320:
+        return [20, 16]
+    if P == 1 and L == 160:
+        return [10, 16]
+    return ct_radices(L)
+
+
 def ct_rounds(L, W, NT):              # tr_nufft.cu: ct_rounds
     return sum(-(-(L // r) * W // NT) for r in ct_radices(L))
 
@@ -67,11 +75,11 @@ def _stage(src, L, W, R, Ns, tw, inv):
     return dst, widx.ravel()
 
 
-def _run(x, L, W, inv, in_place):
+def _run(x, L, W, inv, in_place, plan=0):
     tw = np.exp(-2j * np.pi * np.arange(L) / L)
     buf = x.reshape(-1).astype(np.complex128)
     Ns = 1
-    for R in ct_radices(L):
+    for R in ct_radices_p(plan, L):
         new, widx = _stage(buf, L, W, R, Ns, tw, inv)
         if in_place:
             # every element written exactly once: reads-then-barrier-then-writes is race-free
@@ -92,6 +100,46 @@ def test_schedule_is_the_dft(L, inv, in_place):
     y = _run(x, L, W, inv, in_place)
     ref = np.fft.ifft(x, axis=0) * L if inv else np.fft.fft(x, axis=0)
     assert np.max(np.abs(y - ref)) < 1e-9 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("L", [160, 320])
+@pytest.mark.parametrize("inv", [False, True])
+@pytest.mark.parametrize("in_place", [False, True])
+def test_two_pass_plan_is_the_dft(L, inv, in_place):
+    """Radix plan 1 (20 x 16 at 320, 10 x 16 at 160): the same Stockham indexing
+    and twiddle steps with composite radices give the DFT in two passes."""
+    assert len(ct_radices_p(1, L)) == 2 and int(np.prod(ct_radices_p(1, L))) == L
+    W = 8
+    rng = np.random.default_rng(L + 3 * inv)
+    x = rng.standard_normal((L, W)) + 1j * rng.standard_normal((L, W))
+    y = _run(x, L, W, inv, in_place, plan=1)
+    ref = np.fft.ifft(x, axis=0) * L if inv else np.fft.fft(x, axis=0)
+    assert np.max(np.abs(y - ref)) < 1e-9 * np.max(np.abs(ref))
+
+
+def ct_swz_row(m, sw):                # tr_fft.cuh: ct_swz_row (rows 2i, 2i+1 exchanged in odd blocks)
+    return m ^ ((m // sw) & 1) if sw else m
+
+
+@pytest.mark.parametrize("L", [160, 320])
+def test_two_pass_row_swizzle(L):
+    """With 64-byte rows (W = 8) the first pass's rows R0 j + r of the two
+    butterflies j, j + 1 of a half-warp would share a bank half; the swizzle
+    is a permutation of the tile's rows that gives them opposite halves, and
+    the second pass's rows j + R0 r (consecutive j) stay in opposite halves."""
+    r0, r1 = ct_radices_p(1, L)
+    sw = r0                                        # ct_swz_p: even first radix, 8-column rows
+    assert r0 % 2 == 0
+    rows = [ct_swz_row(m, sw) for m in range(L)]
+    assert sorted(rows) == list(range(L))
+    for j in range(0, L // r0, 2):                 # stage 0: half-warp = butterflies j, j + 1 (8 columns each)
+        for r in range(r0):
+            assert ct_swz_row(r0 * j + r, sw) % 2 != ct_swz_row(r0 * (j + 1) + r, sw) % 2
+    nb = L // r1                                   # stage 1 reads rows j + nb r, nb = r0
+    assert nb == r0
+    for j in range(0, nb, 2):
+        for r in range(r1):
+            assert ct_swz_row(j + nb * r, sw) % 2 != ct_swz_row(j + 1 + nb * r, sw) % 2
 
 
 @pytest.mark.parametrize("L", CT_LENGTHS)

@@ -112,3 +112,39 @@ def test_fused_yz_passes_equal_the_separate_passes(shape, E, C):
     torch.cuda.synchronize()
     assert torch.equal(outs[0][0], outs[1][0])
     assert torch.equal(outs[0][1], outs[1][1])
+
+
+@pytest.mark.parametrize("C,E", [(8, 2), (16, 3)])
+def test_two_pass_x_transforms_match_three_pass(C, E):
+    """The 320-point x passes run in two shared-memory passes (radices 20 x 16,
+    k_fwd_x_wide / k_adj_x_wide) unless TR_PLAN_THREE_PASS_X asks for the three
+    of the other lengths (5, 8, 8).  Both are the same DFT in a different order
+    of float operations: results agree to float rounding (and differ in bits,
+    so the flag does select other kernels), and the two-pass ones match the
+    oracle at the NUFFT bar."""
+    torch = _torch()
+    syn = pkg("synthetic")
+    nb = pkg("nufft_backend")
+    rng = np.random.default_rng(23)
+    shape = (16, 24, 256)                                          # OSX = 320
+    k = syn.cones_trajectory(shape, 256, 200, rng)[:40].reshape(-1, 3)
+    dcf = syn.density(k, shape)
+    mps = syn.coil_maps(shape, C, rng)
+    img = (rng.standard_normal((E,) + shape) + 1j * rng.standard_normal((E,) + shape)).astype(np.complex64)
+    q = (rng.standard_normal((E * C, k.shape[0])) + 1j * rng.standard_normal((E * C, k.shape[0]))).astype(np.complex64)
+    outs = []
+    for three in (False, True):
+        be = nb.B200NufftBackend(shape, [k], 0, dcf=[dcf], n_coils=C, n_echoes=E, three_pass_x=three)
+        be.set_maps(mps)
+        assert be.os_shape[2] == 320
+        fwd = be.unsort_kspace(be.forward_bin(torch.from_numpy(img).cuda(), 0), 0).cpu().numpy()
+        adj = be.adjoint_bin(be.sort_kspace(torch.from_numpy(q).cuda(), 0), 0, use_dcf=True).cpu().numpy()
+        outs.append((fwd.reshape(E, C, -1), adj))
+        be.close()
+    (f2, a2), (f3, a3) = outs
+    assert onf.rel_l2(f2, f3) < 1e-6 and onf.rel_l2(a2, a3) < 1e-6
+    assert not (np.array_equal(f2, f3) and np.array_equal(a2, a3))
+    for e in range(E):
+        assert onf.rel_l2(f2[e], cgrid.nufft(img[e][None] * mps, k)) < TOL_NUFFT
+        ref = np.sum(cgrid.nufft_adjoint(dcf * q.reshape(E, C, -1)[e], k, shape) * np.conj(mps), axis=0)
+        assert onf.rel_l2(a2[e], ref) < TOL_NUFFT
