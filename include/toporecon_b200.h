@@ -72,8 +72,11 @@ typedef struct {
 #define TR_PLAN_NO_TMA 2         /* stage FFT tiles with cp.async instead of TMA (comparison runs) */
 #define TR_PLAN_YZ_FUSION 4      /* run the y and z FFT passes as one cluster kernel where the geometry
                                     allows (comparison runs: measured slower than the separate passes) */
-#define TR_PLAN_THREE_PASS_X 8   /* run the 320-point x transforms in three shared-memory passes
-                                    (radices 5, 8, 8) instead of two (20, 16) (comparison runs) */
+#define TR_PLAN_THREE_PASS_320 8 /* run the 320-point FFT passes (x and the line passes) in three
+                                    shared-memory passes (radices 5, 8, 8) instead of two (20, 16)
+                                    (comparison runs; results agree to float rounding) */
+#define TR_PLAN_NO_COLUMN_SKIP 16 /* transform every z line of the grid, also those of (y, x) tile columns
+                                    that no sample's kernel reaches (comparison runs; same results) */
 
 typedef struct {
     int32_t os_shape[3];         /* oversampled grid (ceil(1.25 n) per axis) */

@@ -25,7 +25,8 @@ TR_ALG = {"tvm": 0, "tvme": 1, "tvmw": 2}
 TR_PLAN_AUTOTUNE = 1
 TR_PLAN_NO_TMA = 2
 TR_PLAN_YZ_FUSION = 4
-TR_PLAN_THREE_PASS_X = 8
+TR_PLAN_THREE_PASS_320 = 8
+TR_PLAN_NO_COLUMN_SKIP = 16
 
 EXPORTED = (
     "tr_plan_create", "tr_plan_destroy", "tr_plan_info", "tr_last_error_string", "tr_plan_set_maps",

@@ -462,11 +462,8 @@ __host__ __device__ constexpr int ct_swz_p(int P, int L, int row_elems) {
     return (P == 1 && ct_nstages_p(P, L) == 2 && ct_radix_p(P, L, 0) % 2 == 0 && row_elems == 8)
                ? ct_radix_p(P, L, 0) : 0;
 }
-template <int SW>
-__device__ __forceinline__ int ct_swz_row(int m) {
-    if constexpr (SW == 0) return m;
-    else return m ^ ((m / SW) & 1);
-}
+// (The map is m -> m ^ ((m / R0) & 1); at the stage 0 writes m / R0 is the
+// butterfly index j, at the stage 1 reads it is the compile-time input index r.)
 
 template <int L, int W, int NT, bool INV, int s, int Ns, bool LD = false, int P = 0>
 struct CtStage {
@@ -492,7 +489,8 @@ struct CtStage {
                 for (int r = 0; r < R; ++r) {
                     float2 x;
                     if constexpr (LD && s == 0) x = load(j + r * NB, w);
-                    else x = src[ct_swz_row<(s == 1 ? SW : 0)>(j + r * NB) * W + w];
+                    // stage 1: row j + NB r with j < NB = SW, so row / SW = r (a constant)
+                    else x = src[((j + r * NB) ^ ((s == 1 && SW) ? (r & 1) : 0)) * W + w];
                     if (Ns > 1 && r > 0) {
                         float2 t = tw[k * r * STEP];
                         if (INV) t.y = -t.y;
@@ -505,7 +503,8 @@ struct CtStage {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     if (s == S - 1) store(d0 + r * Ns, w, v[r]);
-                    else dst[ct_swz_row<(s == 0 ? SW : 0)>(d0 + r * Ns) * W + w] = v[r];
+                    // stage 0: row j SW + r with r < SW, so row / SW = j
+                    else dst[((d0 + r * Ns) ^ ((s == 0 && SW) ? (j & 1) : 0)) * W + w] = v[r];
                 }
             }
         }
@@ -572,7 +571,7 @@ struct CtStageIP {
                 const int k = (Ns == 1) ? 0 : j % Ns;
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    float2 x = buf[ct_swz_row<(s == 1 ? SW : 0)>(j + r * NB) * RS + w];
+                    float2 x = buf[((j + r * NB) ^ ((s == 1 && SW) ? (r & 1) : 0)) * RS + w];
                     if (Ns > 1 && r > 0) {
                         float2 t = tw[k * r * STEP];
                         if (INV) t.y = -t.y;
@@ -595,7 +594,7 @@ struct CtStageIP {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     if (s == S - 1) store(d0 + r * Ns, w, v[it][r]);
-                    else buf[ct_swz_row<(s == 0 ? SW : 0)>(d0 + r * Ns) * RS + w] = v[it][r];
+                    else buf[((d0 + r * Ns) ^ ((s == 0 && SW) ? (j & 1) : 0)) * RS + w] = v[it][r];
                 }
             }
         }
@@ -617,6 +616,10 @@ __device__ __forceinline__ void fft_ct_ip_p(float2* buf, const float2* tw, Store
 template <int L, int W, int RS, int NT, bool INV, class Store>
 __device__ __forceinline__ void fft_ct_ip_rs(float2* buf, const float2* tw, Store& store) {
     CtStageIP<L, W, NT, INV, 0, 1, RS>::run(buf, tw, store);
+}
+template <int P, int L, int W, int RS, int NT, bool INV, class Store>
+__device__ __forceinline__ void fft_ct_ip_rs_p(float2* buf, const float2* tw, Store& store) {
+    CtStageIP<L, W, NT, INV, 0, 1, RS, P>::run(buf, tw, store);
 }
 
 // Buffer that the last stage of an L-point fft_ct does not read.

@@ -162,6 +162,8 @@ struct Bin {
     int64_t list_offset = 0;   // first gather-list entry of the bin
     int64_t list_count = 0;
     int64_t n_busy = 0;        // grid tiles with at least one gather-list entry
+    int64_t n_zero = 0;        // empty tiles in occupied (y, x) tile columns (zero-filled by gridding)
+    int64_t n_occ_cols = 0;    // occupied (y, x) tile columns
     int64_t work_offset = 0;   // first gridding work item of the bin
     int64_t n_work = 0;        // work items: busy tiles, the heaviest split into list ranges
     int64_t split_offset = 0;  // first split-tile record of the bin
@@ -191,7 +193,10 @@ struct tr_plan {
     int32_t* perm = nullptr;     // sorted position -> acquisition index within the bin
     int2* glist = nullptr;          // gridding gather lists: (sample in bin, packed tap offsets), all bins
     int32_t* list_start = nullptr;  // per bin [ntiles + 1] (relative to the bin's first entry)
-    int32_t* tile_order = nullptr;  // per bin [ntiles]: busy tiles heaviest first, then empty tiles
+    int32_t* tile_order = nullptr;  // per bin [ntiles]: busy tiles heaviest first, then the empty tiles of
+                                    // occupied columns, then those of unoccupied columns
+    uint8_t* colmask = nullptr;     // per bin [ntile[1] * ntile[2]]: 1 where some tile of the (y, x) column is busy
+    bool skip_empty_cols = true;    // z passes skip unoccupied columns (not TR_PLAN_NO_COLUMN_SKIP, not fused y + z)
     int4* work = nullptr;           // gridding work items (tile, first entry, end entry, partial slot or -1)
     int4* splits = nullptr;         // split tiles (tile, first partial slot, partial count, 0)
     int ntile[3] = {0, 0, 0};
@@ -220,8 +225,7 @@ struct tr_plan {
     int spread_cols = 128;       // most k-space columns per gridding CTA
     bool use_tma = true;
     bool fuse_yz = false;        // TR_PLAN_YZ_FUSION: fused y + z passes where the geometry allows
-    bool x_two_pass = true;      // 320-point TMA x passes in two shared-memory passes (not TR_PLAN_THREE_PASS_X)
-    bool two_pass_lines[3] = {false, false, false};   // per axis: 160 / 320-point TMA line passes in two passes
+    bool two_pass_320 = true;    // 320-point TMA FFT passes in two shared-memory passes (not TR_PLAN_THREE_PASS_320)
     bool autotune = false;       // TR_PLAN_AUTOTUNE: time launch-shape candidates on first use
     std::map<int, int> spread_cols_tuned;   // column count -> chosen spread_cols         // TMA-tiled FFT passes where the geometry allows
     // TVMW

@@ -179,7 +179,35 @@ struct LineArgs {
     int* err;               // device error word (kDevErr* bits)
     int poll;               // polls before a bounded mbarrier wait gives up
     int kA, kB;             // TMA variant: first transform row of each output box
+    // z passes: (y, x) tile columns that no sample's kernel reaches; null: none skipped
+    const uint8_t* colmask; // [nt1 * nt2] 1: occupied
+    int skip_zero;          // 0: a CTA whose lines are all unoccupied returns (forward: the output is never
+                            // read); 1: it writes zeros to its output rows (adjoint: the lines are zero)
+    int mcol, mosx, mnt2;   // k-space columns, OSX and tile columns along x of the mask
 };
+
+// Empty-column skip of the z passes.  Inner index q of a z pass is
+// ((y OSX + x) ncol + column); a line is unoccupied when the tile column
+// (y / 4, x / 4) holds no busy tile: gridding wrote no tile there (the line is
+// all zeros) and interpolation reads no tap there.  True when every line
+// q0 .. q0 + W - 1 (< inner) of the CTA is unoccupied (the same for all threads).
+__device__ __forceinline__ bool lines_unoccupied(const LineArgs& a, int64_t q0, int W) {
+    if (!a.colmask) return false;
+    const int64_t q1 = min(q0 + W, a.inner) - 1;
+    for (int64_t yx = q0 / a.mcol; yx <= q1 / a.mcol; ++yx) {
+        const int y = (int)(yx / a.mosx), x = (int)(yx - (int64_t)y * a.mosx);
+        if (a.colmask[(y >> 2) * a.mnt2 + (x >> 2)]) return false;
+    }
+    return true;
+}
+// The zeros of an unoccupied CTA's output rows (adjoint z pass): [Lout][W] at q0.
+__device__ __forceinline__ void lines_write_zeros(const LineArgs& a, int64_t q0, int W) {
+    float2* out = a.out + (int64_t)blockIdx.y * a.Lout * a.inner;
+    for (int i = threadIdx.x; i < a.Lout * W; i += blockDim.x) {
+        const int o = i / W, w = i - o * W;
+        if (q0 + w < a.inner) out[(int64_t)o * a.inner + q0 + w] = make_float2(0.f, 0.f);
+    }
+}
 
 // The CTA's [L][W] tile is staged with cp.async (every load in flight at
 // once, zero-filled pad rows and tail columns), then all stages run from
@@ -192,6 +220,10 @@ __global__ void __launch_bounds__(256) k_line(LineArgs a) {
     float2* smB = sm + L * W;
     float2* tws = sm + 2 * L * W;
     const int64_t q0 = (int64_t)blockIdx.x * W;
+    if (lines_unoccupied(a, q0, W)) {
+        if (a.skip_zero) lines_write_zeros(a, q0, W);
+        return;
+    }
     const int64_t outer = blockIdx.y;
     const float2* __restrict__ in = a.in + outer * a.Lin * a.inner;
     float2* __restrict__ out = a.out + outer * a.Lout * a.inner;
@@ -392,6 +424,10 @@ __global__ void __launch_bounds__(256) k_line_ct(LineArgs a) {
     float2* smB = sm + L * W;
     float2* tws = sm + 2 * L * W;
     const int64_t q0 = (int64_t)blockIdx.x * W;
+    if (lines_unoccupied(a, q0, W)) {
+        if (a.skip_zero) lines_write_zeros(a, q0, W);
+        return;
+    }
     const int64_t outer = blockIdx.y;
     const float2* __restrict__ in = a.in + outer * a.Lin * a.inner;
     float2* __restrict__ out = a.out + outer * a.Lout * a.inner;
@@ -463,6 +499,10 @@ __global__ void __launch_bounds__(NT, line_min_ctas(NT, P))
     float2* tws = tsm + L * W;
     const int q0 = (int)blockIdx.x * W;
     const int outer = (int)blockIdx.y;
+    if (lines_unoccupied(a, q0, W)) {                // before any barrier or copy: the CTA leaves whole
+        if (a.skip_zero) lines_write_zeros(a, q0, W);
+        return;
+    }
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -506,8 +546,9 @@ __global__ void __launch_bounds__(NT, line_min_ctas(NT, P))
 //             chunks in flight), the Z cropped rows scattered to the CTAs that
 //             own them, a cluster barrier, then y transforms of its ZR rows and
 //             the Y cropped rows stored by TMA.
-// Each line sees exactly the butterflies, twiddles and order of k_line_tma, so
-// the results equal the separate passes bit for bit.  Reads of the plane all
+// Each line sees exactly the butterflies, twiddles and order of k_line_tma (the
+// two-pass plan at 320 points, the default one at 160), so the results equal the
+// separate passes bit for bit; plans with TR_PLAN_THREE_PASS_320 do not fuse.  Reads of the plane all
 // precede the cluster barrier and writes follow it, so the grid can overwrite
 // the x-pass output of the same plane in place (other clusters touch other
 // (x, column) planes only).  No TMA multicast: every copy is between global
@@ -573,7 +614,7 @@ __global__ void __launch_bounds__(kYzNT, 2) k_yz_fwd(YzArgs a, const __grid_cons
         for (int sub = 0; sub < RS / 16; ++sub) {
             float2* b = ty + sub * 16;
             auto store = [b](int k, int w, float2 v) { b[k * RS + w] = v; };
-            fft_ct_ip_rs<LY, 16, RS, NT, false>(b, twy, store);
+            fft_ct_ip_rs_p<(LY == 320 ? 1 : 0), LY, 16, RS, NT, false>(b, twy, store);
         }
     }
     cluster_sync_all();                     // every y line of the plane is transformed
@@ -694,7 +735,7 @@ __global__ void __launch_bounds__(kYzNT, 2) k_yz_adj(YzArgs a, const __grid_cons
         for (int sub = 0; sub < RS / 16; ++sub) {
             float2* b = ty + sub * 16;
             auto store = [b](int k, int w, float2 v) { b[k * RS + w] = v; };
-            fft_ct_ip_rs<LY, 16, RS, NT, true>(b, twy, store);
+            fft_ct_ip_rs_p<(LY == 320 ? 1 : 0), LY, 16, RS, NT, true>(b, twy, store);
         }
     }
     fence_proxy_async_smem();
@@ -1808,10 +1849,18 @@ static bool line_tma_setup(LineArgs& la, int L, int W, int64_t outer, CUtensorMa
     return true;
 }
 
+// colmask (z passes of bin grids, ncol k-space columns): skip the lines of
+// unoccupied tile columns (inverse: write their zeros), see lines_unoccupied.
 static tr_status launch_line(tr_plan* p, int axis, const float2* in, float2* out, int64_t outer, int64_t inner,
-                             int Lin, int Lout, int p_in, int p_out, bool inv, cudaStream_t st) {
+                             int Lin, int Lout, int p_in, int p_out, bool inv, cudaStream_t st,
+                             const uint8_t* colmask = nullptr, int ncol = 0) {
     const FftAxis& A = p->ax[axis];
     LineArgs la;
+    la.colmask = colmask;
+    la.skip_zero = inv ? 1 : 0;
+    la.mcol = ncol;
+    la.mosx = p->os[2];
+    la.mnt2 = p->ntile[2];
     la.in = in;
     la.out = out;
     la.inner = inner;
@@ -1842,9 +1891,11 @@ static tr_status launch_line(tr_plan* p, int axis, const float2* in, float2* out
     switch (A.L) { TR_CT_LENGTHS(TR_LINE_CASE) default: break; }
 #undef TR_LINE_CASE
     unsigned nt = (unsigned)line_threads(A.L, la.W);
-    if (tma && p->two_pass_lines[axis] && (A.L == 160 || A.L == 320)) {
-        if (A.L == 160) fn = inv ? (const void*)k_line_tma<160, 16, true, 1> : (const void*)k_line_tma<160, 16, false, 1>;
-        else fn = inv ? (const void*)k_line_tma<320, 8, true, 1> : (const void*)k_line_tma<320, 8, false, 1>;
+    // 320-point lines in two passes (radices 20, 16: measured 15 % faster on the y
+    // passes of the 160 x 320 x 320 grid); at 160 the two passes (10, 16: 256 and
+    // 160 butterflies) measured 10 % slower than the three (5, 8, 4) and are not used
+    if (tma && p->two_pass_320 && A.L == 320) {
+        fn = inv ? (const void*)k_line_tma<320, 8, true, 1> : (const void*)k_line_tma<320, 8, false, 1>;
         nt = (unsigned)line_threads_p(A.L, la.W, 1);
     }
     if (!fn) fn = (const void*)k_line;
@@ -1928,7 +1979,7 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
 #define TR_FWDX_TMA(LV) case LV: tfn = (const void*)k_fwd_x_tma<LV, kTmaXWidth>; break;
         switch (OSX) { TR_CT_LENGTHS(TR_FWDX_TMA) default: break; }
 #undef TR_FWDX_TMA
-        if (OSX == 320 && p->x_two_pass) {
+        if (OSX == 320 && p->two_pass_320) {
             tfn = (const void*)k_fwd_x_wide<320, kTmaXWidth>;
             nt = kWideNT;
         }
@@ -1998,6 +2049,7 @@ static tr_status stage_yz(tr_plan* p, int ncol, bool adj, cudaStream_t st, bool*
     *done = false;
     const int Z = p->n[0], Y = p->n[1], OSZ = p->os[0], OSY = p->os[1], OSX = p->os[2];
     if (!p->use_tma || !p->fuse_yz || ncol % kYzCW || Z % 2 || Y % 2 || Y / 2 > 256) return TR_OK;
+    if (OSY == 320 && !p->two_pass_320) return TR_OK;
     const void* fn = nullptr;
     int CL = 0, ZR = 0;
 #define TR_YZ_PICK(LY, LZ, CLV, ZRV)                                                                   \
@@ -2063,10 +2115,16 @@ static tr_status stage_fwd_y(tr_plan* p, int ncol, cudaStream_t st) {
                        false, st);
 }
 
-// z pass: [1][Z -> OSZ][OSY * OSX * ncol]
-static tr_status stage_fwd_z(tr_plan* p, int ncol, cudaStream_t st) {
+// Unoccupied-column mask of a bin for its z passes (null: no skipping).
+static const uint8_t* bin_colmask(const tr_plan* p, int bin) {
+    return (p->skip_empty_cols && p->colmask) ? p->colmask + (int64_t)bin * p->ntile[1] * p->ntile[2] : nullptr;
+}
+
+// z pass: [1][Z -> OSZ][OSY * OSX * ncol]; the lines of unoccupied columns are
+// not computed (interpolation reads none of them)
+static tr_status stage_fwd_z(tr_plan* p, int bin, int ncol, cudaStream_t st) {
     return launch_line(p, 0, p->bufB, p->bufA, 1, (int64_t)p->os[1] * p->os[2] * ncol, p->n[0], p->os[0],
-                       p->ax[0].pad, 0, false, st);
+                       p->ax[0].pad, 0, false, st, bin_colmask(p, bin), ncol);
 }
 
 static tr_status stage_interp(tr_plan* p, int bin, int ncol, int mode, float sigma, const float2* y, float2* out,
@@ -2117,7 +2175,8 @@ static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, 
     sa.tile_order = p->tile_order + (int64_t)bin * p->ntiles;
     sa.work = p->work + b.work_offset;
     sa.n_busy = (int)b.n_busy;
-    sa.n_empty = (int)(p->ntiles - b.n_busy);
+    // zero tiles: only those of occupied columns when the z pass skips the rest
+    sa.n_empty = (int)(bin_colmask(p, bin) ? b.n_zero : p->ntiles - b.n_busy);
     sa.n_work = (int)b.n_work;
     sa.partials = p->bufB;     // free during gridding (the adjoint z pass fills it afterwards)
     sa.vals = ksp;
@@ -2169,10 +2228,11 @@ static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, 
     return TR_OK;
 }
 
-// z pass (inverse, crop to Z): [1][OSZ -> Z][OSY * OSX * ncol]
-static tr_status stage_adj_z(tr_plan* p, int ncol, cudaStream_t st) {
+// z pass (inverse, crop to Z): [1][OSZ -> Z][OSY * OSX * ncol]; the lines of
+// unoccupied columns (gridding left them unwritten: they are zero) give zeros
+static tr_status stage_adj_z(tr_plan* p, int bin, int ncol, cudaStream_t st) {
     return launch_line(p, 0, p->bufA, p->bufB, 1, (int64_t)p->os[1] * p->os[2] * ncol, p->os[0], p->n[0], 0,
-                       p->ax[0].pad, true, st);
+                       p->ax[0].pad, true, st, bin_colmask(p, bin), ncol);
 }
 
 // y pass (inverse, crop to Y): [Z][OSY -> Y][OSX * ncol]
@@ -2229,7 +2289,7 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
         switch (OSX) { TR_CT_LENGTHS(TR_ADJX_TMA) default: break; }
 #undef TR_ADJX_TMA
         unsigned nt = (unsigned)ct_threads(OSX, kTmaXWidth);
-        if (OSX == 320 && p->x_two_pass && X % 16 == 0) {  // X <= 256: kWideXBlocks blocks of 16 per warp
+        if (OSX == 320 && p->two_pass_320 && X % 16 == 0) {  // X <= 256: kWideXBlocks blocks of 16 per warp
             tfn = (const void*)k_adj_x_wide<320, kTmaXWidth>;
             nt = kWideNT;
         }
@@ -2277,7 +2337,7 @@ tr_status nufft_forward_cols(tr_plan* p, int bin, const float2* images, int64_t 
     TR_TRY(stage_yz(p, ncol, false, st, &fused));
     if (!fused) {
         TR_TRY(stage_fwd_y(p, ncol, st));
-        TR_TRY(stage_fwd_z(p, ncol, st));
+        TR_TRY(stage_fwd_z(p, bin, ncol, st));
     }
     return stage_interp(p, bin, ncol, mode, sigma, y, out, st);
 }
@@ -2340,7 +2400,7 @@ tr_status nufft_adjoint_cols(tr_plan* p, int bin, const float2* ksp, int n_img, 
     bool fused = false;
     TR_TRY(stage_yz(p, ncol, true, st, &fused));
     if (!fused) {
-        TR_TRY(stage_adj_z(p, ncol, st));
+        TR_TRY(stage_adj_z(p, bin, ncol, st));
         TR_TRY(stage_adj_y(p, ncol, st));
     }
     return stage_adj_x(p, n_img, maps, C, images, img_stride, st);
@@ -2368,10 +2428,16 @@ tr_status profile_nufft(tr_plan* p, int bin, int reps, double* ms, double* bytes
     TR_TRY(tune_spread_cols(p, bin, ksp, ncol, true, st));
     bytes[0] = c8 * (E * N + C * N + XP * ncol);
     bytes[1] = c8 * ncol * (XP + YP);
-    bytes[2] = c8 * ncol * (YP + G);
+    // z passes with the empty-column skip: only the occupied lines are read (and,
+    // forward, written); gridding writes the busy and zero-filled tiles only
+    const Bin& bb = p->bins[bin];
+    const bool skip = bin_colmask(p, bin) != nullptr;
+    const double fo = skip ? (double)bb.n_occ_cols / ((double)p->ntile[1] * p->ntile[2]) : 1.0;
+    const double fg = skip ? (double)(bb.n_busy + bb.n_zero) / (double)p->ntiles : 1.0;
+    bytes[2] = c8 * ncol * fo * (YP + G);
     bytes[3] = c8 * (G * ncol + 3 * M * ncol) + 16.0 * M;
-    bytes[4] = c8 * (M * ncol + G * ncol) + 16.0 * M;
-    bytes[5] = c8 * ncol * (G + YP);
+    bytes[4] = c8 * (M * ncol + fg * G * ncol) + 16.0 * M;
+    bytes[5] = c8 * ncol * (fo * G + YP);
     bytes[6] = c8 * ncol * (YP + XP);
     bytes[7] = c8 * (XP * ncol + C * N + E * N);
     bytes[8] = c8 * ncol * (XP + G);      // fused forward y + z
@@ -2387,10 +2453,10 @@ tr_status profile_nufft(tr_plan* p, int bin, int reps, double* ms, double* bytes
             switch (s) {
                 case 0: return stage_fwd_x(p, img, N, E, p->maps, C, st);
                 case 1: return stage_fwd_y(p, ncol, st);
-                case 2: return stage_fwd_z(p, ncol, st);
+                case 2: return stage_fwd_z(p, bin, ncol, st);
                 case 3: return stage_interp(p, bin, ncol, kInterpDualProx, 1.f / 6.f, yk, ksp, st);
                 case 4: return stage_spread(p, bin, ksp, ncol, true, st);
-                case 5: return stage_adj_z(p, ncol, st);
+                case 5: return stage_adj_z(p, bin, ncol, st);
                 case 6: return stage_adj_y(p, ncol, st);
                 case 7: return stage_adj_x(p, E, p->maps, C, img, N, st);
                 case 8: return stage_yz(p, ncol, false, st, &fused);
@@ -2447,6 +2513,7 @@ static void plan_free(tr_plan* p) {
     cudaFree(p->splits);
     cudaFree(p->list_start);
     cudaFree(p->tile_order);
+    cudaFree(p->colmask);
     cudaFree(p->maps);
     cudaFree(p->bufA);
     cudaFree(p->bufB);
@@ -2491,9 +2558,10 @@ static int axis_tiles(float k, int os, int* tile, int* rel) {
 // grid tile the samples whose support meets it, in sorted-sample order, as
 // (sample, packed tap offsets); list_start [ntiles + 1] relative to the bin's
 // first entry; order: busy tiles by entry count (heaviest first, stable),
-// then the empty tiles.
+// then the empty tiles of occupied (y, x) tile columns, then the rest;
+// colmask [ntile[1] * ntile[2]]: 1 for the occupied columns.
 static tr_status build_gather_lists(tr_plan* p, int bin, const float4* ks, int64_t M, std::vector<int2>& glist,
-                                    int32_t* list_start, int32_t* order, std::vector<int4>& work,
+                                    int32_t* list_start, int32_t* order, uint8_t* colmask, std::vector<int4>& work,
                                     std::vector<int4>& splits) {
     const int64_t nt = p->ntiles;
     std::vector<int64_t> cnt((size_t)nt + 1, 0);
@@ -2523,12 +2591,18 @@ static tr_status build_gather_lists(tr_plan* p, int bin, const float4* ks, int64
     std::vector<int64_t> cur(cnt.begin(), cnt.end() - 1);
     visit([&](int64_t t, int32_t m, int packed) { dst[cur[(size_t)t]++] = make_int2(m, packed); });
     std::vector<std::pair<int64_t, int32_t>> busy;
-    std::vector<int32_t> empty;
+    std::vector<int32_t> empty, unoccupied;
+    const int64_t ncolumns = (int64_t)p->ntile[1] * p->ntile[2];
+    std::fill(colmask, colmask + ncolumns, (uint8_t)0);
+    for (int64_t t = 0; t < nt; ++t)
+        if (cnt[(size_t)t + 1] > cnt[(size_t)t]) colmask[t % ncolumns] = 1;   // t = tz * ncolumns + column
+    B.n_occ_cols = std::count(colmask, colmask + ncolumns, (uint8_t)1);
     for (int64_t t = 0; t < nt; ++t) {
         list_start[t] = (int32_t)cnt[(size_t)t];
         const int64_t c = cnt[(size_t)t + 1] - cnt[(size_t)t];
         if (c > 0) busy.push_back({-c, (int32_t)t});
-        else empty.push_back((int32_t)t);
+        else if (colmask[t % ncolumns]) empty.push_back((int32_t)t);
+        else unoccupied.push_back((int32_t)t);
     }
     list_start[nt] = (int32_t)total;
     std::stable_sort(busy.begin(), busy.end(),
@@ -2536,8 +2610,10 @@ static tr_status build_gather_lists(tr_plan* p, int bin, const float4* ks, int64
                          return x.first < y.first;
                      });
     B.n_busy = (int64_t)busy.size();
+    B.n_zero = (int64_t)empty.size();
     for (size_t i = 0; i < busy.size(); ++i) order[i] = busy[i].second;
     for (size_t i = 0; i < empty.size(); ++i) order[busy.size() + i] = empty[i];
+    for (size_t i = 0; i < unoccupied.size(); ++i) order[busy.size() + empty.size() + i] = unoccupied[i];
     // work items: lists longer than `split` entries become ranges of `split`;
     // their partial tiles (64 points x ncol) live in the y-pass buffer, which
     // holds n[0] * os[1] * os[2] points per column, so the split is widened
@@ -2653,6 +2729,8 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
     std::vector<int32_t> perm((size_t)std::max<int64_t>(off, 1));
     std::vector<int32_t> lstart((size_t)(p->ntiles + 1) * d->n_bins);
     std::vector<int32_t> torder((size_t)p->ntiles * d->n_bins);
+    const size_t ncolumns = (size_t)p->ntile[1] * p->ntile[2];
+    std::vector<uint8_t> cmask(ncolumns * d->n_bins);
     std::vector<int2> glist;
     std::vector<int4> gwork, gsplits;
     float scale[3], shift[3];
@@ -2708,8 +2786,8 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
         }
         // gather lists: every (tile, sample) pair where the sample's KB support meets the tile
         out.rc = build_gather_lists(p, b, M ? &ks_sorted[(size_t)o] : nullptr, M, out.glist,
-                                    &lstart[(size_t)b * (p->ntiles + 1)], &torder[(size_t)b * p->ntiles], out.work,
-                                    out.splits);
+                                    &lstart[(size_t)b * (p->ntiles + 1)], &torder[(size_t)b * p->ntiles],
+                                    &cmask[(size_t)b * ncolumns], out.work, out.splits);
         if (out.rc != TR_OK) out.msg = g_last_error;     // this worker thread's message
     };
     {
@@ -2751,7 +2829,8 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
         cudaMalloc(&p->list_start, lstart.size() * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&p->work, std::max<size_t>(gwork.size(), 1) * sizeof(int4)) != cudaSuccess ||
         cudaMalloc(&p->splits, std::max<size_t>(gsplits.size(), 1) * sizeof(int4)) != cudaSuccess ||
-        cudaMalloc(&p->tile_order, torder.size() * sizeof(int32_t)) != cudaSuccess)
+        cudaMalloc(&p->tile_order, torder.size() * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&p->colmask, cmask.size()) != cudaSuccess)
         return bad(TR_ERR_OOM, "allocation of the sorted trajectory failed");
     TR_CUDA(cudaMemcpy(p->ks, ks_sorted.data(), nks * sizeof(float4), cudaMemcpyHostToDevice));
     TR_CUDA(cudaMemcpy(p->perm, perm.data(), nks * sizeof(int32_t), cudaMemcpyHostToDevice));
@@ -2766,6 +2845,7 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
     if (!gsplits.empty())
         TR_CUDA(cudaMemcpy(p->splits, gsplits.data(), gsplits.size() * sizeof(int4), cudaMemcpyHostToDevice));
     TR_CUDA(cudaMemcpy(p->tile_order, torder.data(), torder.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    TR_CUDA(cudaMemcpy(p->colmask, cmask.data(), cmask.size(), cudaMemcpyHostToDevice));
     if (cudaMalloc(&p->tol_dev, 4 * sizeof(double)) != cudaSuccess ||
         cudaMallocHost(&p->tol_host, 4 * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&p->dev_err, sizeof(int)) != cudaSuccess || cudaMallocHost(&p->err_host, sizeof(int)) != cudaSuccess)
@@ -2774,11 +2854,13 @@ static tr_status plan_create_impl(const tr_plan_desc* d, tr_plan** out) {
     *p->err_host = 0;
     p->use_tma = (d->flags & TR_PLAN_NO_TMA) == 0;
     p->fuse_yz = (d->flags & TR_PLAN_YZ_FUSION) != 0;
-    p->x_two_pass = (d->flags & TR_PLAN_THREE_PASS_X) == 0;
+    p->two_pass_320 = (d->flags & TR_PLAN_THREE_PASS_320) == 0;
+    // the fused y + z kernels transform every line: gridding then zero-fills every empty tile
+    p->skip_empty_cols = (d->flags & TR_PLAN_NO_COLUMN_SKIP) == 0 && !p->fuse_yz;
     p->autotune = (d->flags & TR_PLAN_AUTOTUNE) != 0;
     p->workspace_bytes = (int64_t)(nks * (sizeof(float4) + sizeof(TapRec) + sizeof(int32_t)) +
                                    glist.size() * sizeof(int2) + (gwork.size() + gsplits.size()) * sizeof(int4) +
-                                   (lstart.size() + torder.size()) * sizeof(int32_t));
+                                   (lstart.size() + torder.size()) * sizeof(int32_t) + cmask.size());
     TR_TRY(wavelet_prepare(p));
     owner.p = nullptr;
     *out = p;

@@ -115,13 +115,15 @@ class B200NufftBackend(NufftBackend):
     coordinates, device)`` (``nufft_backend.py:58-88``);
     ``dcf`` (per-bin density weights), ``n_coils`` and ``n_echoes`` configure
     the batched path used by the b200 reconstructors.  ``tma``, ``fuse_yz`` and
-    ``three_pass_x`` select kernel variants for comparison runs (TR_PLAN_NO_TMA,
-    TR_PLAN_YZ_FUSION, TR_PLAN_THREE_PASS_X); results agree to float rounding.
+    ``three_pass_320`` select kernel variants for comparison runs (TR_PLAN_NO_TMA,
+    TR_PLAN_YZ_FUSION, TR_PLAN_THREE_PASS_320); results agree to float rounding.
+    ``column_skip=False`` (TR_PLAN_NO_COLUMN_SKIP) makes the z passes transform
+    the grid lines of (y, x) tile columns no sample reaches as well (same bits).
     """
 
     def __init__(self, img_shape, coordinates, device=0, *, dcf: Iterable | None = None, n_coils: int = 1,
                  n_echoes: int = 1, autotune: bool = False, tma: bool = True, fuse_yz: bool = False,
-                 three_pass_x: bool = False) -> None:
+                 three_pass_320: bool = False, column_skip: bool = True) -> None:
         super().__init__(img_shape)
         import torch
         self._torch = torch
@@ -163,7 +165,8 @@ class B200NufftBackend(NufftBackend):
         desc.width = 4
         desc.device = self.device_index
         desc.flags = ((_lib.TR_PLAN_AUTOTUNE if autotune else 0) | (0 if tma else _lib.TR_PLAN_NO_TMA)
-                      | (_lib.TR_PLAN_YZ_FUSION if fuse_yz else 0) | (_lib.TR_PLAN_THREE_PASS_X if three_pass_x else 0))
+                      | (_lib.TR_PLAN_YZ_FUSION if fuse_yz else 0) | (_lib.TR_PLAN_THREE_PASS_320 if three_pass_320 else 0)
+                      | (0 if column_skip else _lib.TR_PLAN_NO_COLUMN_SKIP))
         handle = ctypes.c_void_p()
         _lib.check(lib.tr_plan_create(ctypes.byref(desc), ctypes.byref(handle)), "tr_plan_create")
         self._plan = handle

@@ -39,8 +39,10 @@ def main(argv=None):
     ap.add_argument("--bins", type=int, default=2)
     ap.add_argument("--no-tma", action="store_true", help="stage the FFT passes with cp.async instead of TMA")
     ap.add_argument("--fuse-yz", action="store_true", help="also time the fused y + z cluster kernels")
-    ap.add_argument("--three-pass-x", action="store_true",
-                    help="run the 320-point x transforms in three shared-memory passes (radices 5, 8, 8)")
+    ap.add_argument("--three-pass-320", action="store_true",
+                    help="run the 320-point transforms in three shared-memory passes (radices 5, 8, 8)")
+    ap.add_argument("--no-column-skip", action="store_true",
+                    help="transform the z lines of (y, x) tile columns that no sample reaches as well")
     ap.add_argument("--autotune", action="store_true", help="let the plan time its launch-shape candidates")
     args = ap.parse_args(argv)
     import torch
@@ -52,7 +54,7 @@ def main(argv=None):
     dcf = syn.density(coord, shape)
     be = nb.B200NufftBackend(shape, [coord], 0, dcf=[dcf], n_coils=args.coils, n_echoes=args.echoes,
                              tma=not args.no_tma, autotune=args.autotune, fuse_yz=args.fuse_yz,
-                             three_pass_x=args.three_pass_x)
+                             three_pass_320=args.three_pass_320, column_skip=not args.no_column_skip)
     mps = syn.coil_maps(shape, args.coils, rng)
     be.set_maps(mps)
     prof = be.profile(0, reps=args.reps)

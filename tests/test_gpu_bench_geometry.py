@@ -115,18 +115,19 @@ def test_fused_yz_passes_equal_the_separate_passes(shape, E, C):
 
 
 @pytest.mark.parametrize("C,E", [(8, 2), (16, 3)])
-def test_two_pass_x_transforms_match_three_pass(C, E):
-    """The 320-point x passes run in two shared-memory passes (radices 20 x 16,
-    k_fwd_x_wide / k_adj_x_wide) unless TR_PLAN_THREE_PASS_X asks for the three
-    of the other lengths (5, 8, 8).  Both are the same DFT in a different order
-    of float operations: results agree to float rounding (and differ in bits,
-    so the flag does select other kernels), and the two-pass ones match the
-    oracle at the NUFFT bar."""
+def test_two_pass_320_transforms_match_three_pass(C, E):
+    """The 320-point FFT passes (here the x passes, k_fwd_x_wide / k_adj_x_wide,
+    and the y passes, k_line_tma with radix plan 1) run in two shared-memory
+    passes (radices 20 x 16) unless TR_PLAN_THREE_PASS_320 asks for the three of
+    the other lengths (5, 8, 8).  Both are the same DFT in a different order of
+    float operations: results agree to float rounding (and differ in bits, so
+    the flag does select other kernels), and the two-pass ones match the oracle
+    at the NUFFT bar."""
     torch = _torch()
     syn = pkg("synthetic")
     nb = pkg("nufft_backend")
     rng = np.random.default_rng(23)
-    shape = (16, 24, 256)                                          # OSX = 320
+    shape = (16, 256, 256)                                         # OSY = OSX = 320
     k = syn.cones_trajectory(shape, 256, 200, rng)[:40].reshape(-1, 3)
     dcf = syn.density(k, shape)
     mps = syn.coil_maps(shape, C, rng)
@@ -134,9 +135,9 @@ def test_two_pass_x_transforms_match_three_pass(C, E):
     q = (rng.standard_normal((E * C, k.shape[0])) + 1j * rng.standard_normal((E * C, k.shape[0]))).astype(np.complex64)
     outs = []
     for three in (False, True):
-        be = nb.B200NufftBackend(shape, [k], 0, dcf=[dcf], n_coils=C, n_echoes=E, three_pass_x=three)
+        be = nb.B200NufftBackend(shape, [k], 0, dcf=[dcf], n_coils=C, n_echoes=E, three_pass_320=three)
         be.set_maps(mps)
-        assert be.os_shape[2] == 320
+        assert be.os_shape[1:] == (320, 320)
         fwd = be.unsort_kspace(be.forward_bin(torch.from_numpy(img).cuda(), 0), 0).cpu().numpy()
         adj = be.adjoint_bin(be.sort_kspace(torch.from_numpy(q).cuda(), 0), 0, use_dcf=True).cpu().numpy()
         outs.append((fwd.reshape(E, C, -1), adj))
@@ -148,3 +149,35 @@ def test_two_pass_x_transforms_match_three_pass(C, E):
         assert onf.rel_l2(f2[e], cgrid.nufft(img[e][None] * mps, k)) < TOL_NUFFT
         ref = np.sum(cgrid.nufft_adjoint(dcf * q.reshape(E, C, -1)[e], k, shape) * np.conj(mps), axis=0)
         assert onf.rel_l2(a2[e], ref) < TOL_NUFFT
+
+
+def test_empty_column_skip_gives_the_same_bits():
+    """The z passes leave out the grid lines of (y, x) tile columns that no
+    sample's kernel reaches: forward, interpolation never reads them; adjoint,
+    gridding writes no tile there and the pass writes their zeros.  On a
+    trajectory that leaves most columns empty (64 cones of the benchmark's
+    4096) the NUFFT results equal those of a plan that transforms every line
+    (TR_PLAN_NO_COLUMN_SKIP) bit for bit, and the per-stage bytes count only
+    the occupied lines."""
+    torch = _torch()
+    syn = pkg("synthetic")
+    nb = pkg("nufft_backend")
+    rng = np.random.default_rng(31)
+    shape, E, C = (64, 96, 96), 2, 8
+    k = syn.cones_trajectory(shape, 4096, 300, rng)[:64].reshape(-1, 3)
+    dcf = syn.density(k, shape)
+    mps = syn.coil_maps(shape, C, rng)
+    img = torch.randn((E,) + shape, dtype=torch.complex64, device="cuda")
+    q = torch.randn((k.shape[0], E * C), dtype=torch.complex64, device="cuda")
+    outs, prof = [], []
+    for skip in (True, False):
+        be = nb.B200NufftBackend(shape, [k], 0, dcf=[dcf], n_coils=C, n_echoes=E, column_skip=skip)
+        be.set_maps(mps)
+        prof.append(be.profile(0, reps=1))
+        outs.append((be.forward_bin(img, 0).clone(), be.adjoint_bin(q, 0, use_dcf=True).clone()))
+        be.close()
+    torch.cuda.synchronize()
+    assert torch.equal(outs[0][0], outs[1][0])
+    assert torch.equal(outs[0][1], outs[1][1])
+    assert prof[0]["fwd_z"]["bytes"] < prof[1]["fwd_z"]["bytes"]
+    assert prof[0]["adj_z"]["bytes"] < prof[1]["adj_z"]["bytes"]
