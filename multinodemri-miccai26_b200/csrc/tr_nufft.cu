@@ -191,6 +191,8 @@ struct LineArgs {
 // (y / 4, x / 4) holds no busy tile: gridding wrote no tile there (the line is
 // all zeros) and interpolation reads no tap there.  True when every line
 // q0 .. q0 + W - 1 (< inner) of the CTA is unoccupied (the same for all threads).
+// The host passes a mask only when W divides ncol, so a CTA never mixes lines
+// of occupied and unoccupied columns (it would read unwritten tiles).
 __device__ __forceinline__ bool lines_unoccupied(const LineArgs& a, int64_t q0, int W) {
     if (!a.colmask) return false;
     const int64_t q1 = min(q0 + W, a.inner) - 1;
@@ -2115,16 +2117,32 @@ static tr_status stage_fwd_y(tr_plan* p, int ncol, cudaStream_t st) {
                        false, st);
 }
 
-// Unoccupied-column mask of a bin for its z passes (null: no skipping).
-static const uint8_t* bin_colmask(const tr_plan* p, int bin) {
-    return (p->skip_empty_cols && p->colmask) ? p->colmask + (int64_t)bin * p->ntile[1] * p->ntile[2] : nullptr;
+static bool ct_compiled(int L) {
+    switch (L) {
+#define TR_CT_CASE_TRUE(LV) case LV: return true;
+        TR_CT_LENGTHS(TR_CT_CASE_TRUE)
+#undef TR_CT_CASE_TRUE
+        default: return false;
+    }
+}
+
+// Unoccupied-column mask of a bin for its z passes and its gridding (null: no
+// skipping).  Gridding leaves the tiles of unoccupied columns unwritten only
+// when no z-pass CTA mixes lines of occupied and unoccupied columns (a mixed
+// CTA transforms all its lines): every CTA's W lines lie in one (y, x) column
+// when ncol is a multiple of the z pass's W (16 at the compiled lengths, the
+// runtime-radix width elsewhere).
+static const uint8_t* bin_colmask(const tr_plan* p, int bin, int ncol) {
+    const int zw = ct_compiled(p->os[0]) ? ct_width(p->os[0]) : p->line_width;
+    if (!p->skip_empty_cols || !p->colmask || ncol % zw) return nullptr;
+    return p->colmask + (int64_t)bin * p->ntile[1] * p->ntile[2];
 }
 
 // z pass: [1][Z -> OSZ][OSY * OSX * ncol]; the lines of unoccupied columns are
 // not computed (interpolation reads none of them)
 static tr_status stage_fwd_z(tr_plan* p, int bin, int ncol, cudaStream_t st) {
     return launch_line(p, 0, p->bufB, p->bufA, 1, (int64_t)p->os[1] * p->os[2] * ncol, p->n[0], p->os[0],
-                       p->ax[0].pad, 0, false, st, bin_colmask(p, bin), ncol);
+                       p->ax[0].pad, 0, false, st, bin_colmask(p, bin, ncol), ncol);
 }
 
 static tr_status stage_interp(tr_plan* p, int bin, int ncol, int mode, float sigma, const float2* y, float2* out,
@@ -2176,7 +2194,7 @@ static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, 
     sa.work = p->work + b.work_offset;
     sa.n_busy = (int)b.n_busy;
     // zero tiles: only those of occupied columns when the z pass skips the rest
-    sa.n_empty = (int)(bin_colmask(p, bin) ? b.n_zero : p->ntiles - b.n_busy);
+    sa.n_empty = (int)(bin_colmask(p, bin, ncol) ? b.n_zero : p->ntiles - b.n_busy);
     sa.n_work = (int)b.n_work;
     sa.partials = p->bufB;     // free during gridding (the adjoint z pass fills it afterwards)
     sa.vals = ksp;
@@ -2232,7 +2250,7 @@ static tr_status stage_spread(tr_plan* p, int bin, const float2* ksp, int ncol, 
 // unoccupied columns (gridding left them unwritten: they are zero) give zeros
 static tr_status stage_adj_z(tr_plan* p, int bin, int ncol, cudaStream_t st) {
     return launch_line(p, 0, p->bufA, p->bufB, 1, (int64_t)p->os[1] * p->os[2] * ncol, p->os[0], p->n[0], 0,
-                       p->ax[0].pad, true, st, bin_colmask(p, bin), ncol);
+                       p->ax[0].pad, true, st, bin_colmask(p, bin, ncol), ncol);
 }
 
 // y pass (inverse, crop to Y): [Z][OSY -> Y][OSX * ncol]
@@ -2431,7 +2449,7 @@ tr_status profile_nufft(tr_plan* p, int bin, int reps, double* ms, double* bytes
     // z passes with the empty-column skip: only the occupied lines are read (and,
     // forward, written); gridding writes the busy and zero-filled tiles only
     const Bin& bb = p->bins[bin];
-    const bool skip = bin_colmask(p, bin) != nullptr;
+    const bool skip = bin_colmask(p, bin, ncol) != nullptr;
     const double fo = skip ? (double)bb.n_occ_cols / ((double)p->ntile[1] * p->ntile[2]) : 1.0;
     const double fg = skip ? (double)(bb.n_busy + bb.n_zero) / (double)p->ntiles : 1.0;
     bytes[2] = c8 * ncol * fo * (YP + G);

@@ -151,20 +151,23 @@ def test_two_pass_320_transforms_match_three_pass(C, E):
         assert onf.rel_l2(a2[e], ref) < TOL_NUFFT
 
 
-def test_empty_column_skip_gives_the_same_bits():
+@pytest.mark.parametrize("shape,cones,E,C", [((64, 96, 96), 64, 2, 8), ((16, 20, 24), 24, 2, 8), ((16, 20, 24), 24, 2, 3)])
+def test_empty_column_skip_gives_the_same_bits(shape, cones, E, C):
     """The z passes leave out the grid lines of (y, x) tile columns that no
     sample's kernel reaches: forward, interpolation never reads them; adjoint,
     gridding writes no tile there and the pass writes their zeros.  On a
     trajectory that leaves most columns empty (64 cones of the benchmark's
     4096) the NUFFT results equal those of a plan that transforms every line
     (TR_PLAN_NO_COLUMN_SKIP) bit for bit, and the per-stage bytes count only
-    the occupied lines."""
+    the occupied lines.  Cases: the compiled z length (TMA pass), a runtime-
+    radix one (odd grid, 20 x 25 x 30), and a column count (6) that is not a
+    multiple of the z pass's 16 lines per CTA, where a CTA would mix occupied
+    and unoccupied columns and the plan does not skip."""
     torch = _torch()
     syn = pkg("synthetic")
     nb = pkg("nufft_backend")
     rng = np.random.default_rng(31)
-    shape, E, C = (64, 96, 96), 2, 8
-    k = syn.cones_trajectory(shape, 4096, 300, rng)[:64].reshape(-1, 3)
+    k = syn.cones_trajectory(shape, 4096, 300, rng)[:cones].reshape(-1, 3)
     dcf = syn.density(k, shape)
     mps = syn.coil_maps(shape, C, rng)
     img = torch.randn((E,) + shape, dtype=torch.complex64, device="cuda")
@@ -179,5 +182,8 @@ def test_empty_column_skip_gives_the_same_bits():
     torch.cuda.synchronize()
     assert torch.equal(outs[0][0], outs[1][0])
     assert torch.equal(outs[0][1], outs[1][1])
-    assert prof[0]["fwd_z"]["bytes"] < prof[1]["fwd_z"]["bytes"]
-    assert prof[0]["adj_z"]["bytes"] < prof[1]["adj_z"]["bytes"]
+    if (E * C) % 16 == 0:
+        assert prof[0]["fwd_z"]["bytes"] < prof[1]["fwd_z"]["bytes"]
+        assert prof[0]["adj_z"]["bytes"] < prof[1]["adj_z"]["bytes"]
+    else:
+        assert prof[0]["fwd_z"]["bytes"] == prof[1]["fwd_z"]["bytes"]
