@@ -70,8 +70,8 @@ WARM_MATCH = 1e-3      # warm-started result must match the plain result to this
 # 96-column bench workload is these figures x ncol / 16.
 NCU_TRAFFIC_16COL = {
     "workload": "tvme-256", "columns": 16,
-    "fwd_x": 1.962e9, "fwd_y": 2.974e9, "fwd_z": 3.723e9, "interp": 1.303e9,
-    "spread": 2.296e9, "adj_z": 3.732e9, "adj_y": 2.984e9, "adj_x": 2.012e9,
+    "fwd_x": 1.962e9, "fwd_y": 2.973e9, "fwd_z": 3.019e9, "interp": 1.304e9,
+    "spread": 2.296e9, "adj_z": 3.326e9, "adj_y": 2.982e9, "adj_x": 2.012e9,
 }
 
 # Iterations to --tol of plain PDHG with the reference's steps (sigma = tau =
