@@ -1571,7 +1571,9 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : (CG >= 4 ? 4 : 5))) k_spre
 
     const int row = tid >> 4;          // tile row (z, y) = (row / 4, row % 4)
     const int g = tid & 15;
-    const int c_lo = g * CG;
+    // columns g + 16 j (j < CG): a half-warp (one tile row) reads 16 consecutive
+    // values of an entry per load, one 128-byte wavefront (with g CG + j the
+    // 8 CG-byte stride put groups g and g + 8 on the same banks)
     float2 acc[4][CG];
 #pragma unroll
     for (int x = 0; x < 4; ++x)
@@ -1643,7 +1645,7 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : (CG >= 4 ? 4 : 5))) k_spre
             const float wx[4] = {wx4.x, wx4.y, wx4.z, wx4.w};
             float2 v[CG];
 #pragma unroll
-            for (int j = 0; j < CG; ++j) v[j] = (c_lo + j < ncc) ? dq[cc * cst + c_lo + j] : make_float2(0.f, 0.f);
+            for (int j = 0; j < CG; ++j) v[j] = (g + 16 * j < ncc) ? dq[cc * cst + g + 16 * j] : make_float2(0.f, 0.f);
 #pragma unroll
             for (int x = 0; x < 4; ++x) {
                 if (wx[x] == 0.f) continue;
@@ -1668,7 +1670,7 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : (CG >= 4 ? 4 : 5))) k_spre
             for (int x = 0; x < 4; ++x)
 #pragma unroll
                 for (int j = 0; j < CG; ++j)
-                    if (c_lo + j < ncc) dq[((row % kPieceRows) * 4 + x) * cst + c_lo + j] = acc[x][j];
+                    if (g + 16 * j < ncc) dq[((row % kPieceRows) * 4 + x) * cst + g + 16 * j] = acc[x][j];
         }
         if (TMA && slot < 0) {
             fence_proxy_async_smem();
