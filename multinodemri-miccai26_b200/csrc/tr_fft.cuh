@@ -520,10 +520,10 @@ struct CtStage {
 struct NoLoad {
     __device__ __forceinline__ float2 operator()(int, int) const { return make_float2(0.f, 0.f); }
 };
-template <int L, int W, int NT, bool INV, class Store, int P = 0>
+template <int L, int W, int NT, bool INV, class Store>
 __device__ __forceinline__ void fft_ct(float2* A, float2* B, const float2* tw, Store& store) {
     NoLoad none;
-    CtStage<L, W, NT, INV, 0, 1, false, P>::run(A, B, tw, none, store);
+    CtStage<L, W, NT, INV, 0, 1>::run(A, B, tw, none, store);
 }
 template <int P, int L, int W, int NT, bool INV, class Store>
 __device__ __forceinline__ void fft_ct_p(float2* A, float2* B, const float2* tw, Store& store) {

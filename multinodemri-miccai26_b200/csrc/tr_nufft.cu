@@ -1232,8 +1232,10 @@ __global__ void __launch_bounds__(kWideNT, 5) k_fwd_x_wide(FwdXArgs a, const __g
 // Epilogue: lane l of a warp takes image column x = 16 b + l / 2 of block b
 // (blocks dealt to the warps in turn) and coils 4 (l % 2) .. 4 (l % 2) + 3 of
 // the group, so a warp's coil-map loads cover 1 KB in 8 (C = 8) or 16 lines
-// instead of one 64-byte piece per thread in 32; the two lanes of a column add
-// their products with one butterfly shuffle (the same sum in both lanes).
+// instead of one 64-byte piece per thread in 32.  The two lanes of a column
+// exchange one component each (one shuffle): the even lane keeps the real part
+// of the column's sum, the odd lane the imaginary part, and each writes its
+// float of the result (a warp's stores are 128 contiguous bytes).
 constexpr int kWideXBlocks = 4;               // ceil(256 / 16 / (kWideNT / 32)): X <= 256
 
 template <int L, int W>
