@@ -203,8 +203,8 @@ __device__ __forceinline__ bool lines_unoccupied(const LineArgs& a, int64_t q0, 
     return true;
 }
 // The zeros of an unoccupied CTA's output rows (adjoint z pass): [Lout][W] at q0.
-__device__ __forceinline__ void lines_write_zeros(const LineArgs& a, int64_t q0, int W) {
-    float2* out = a.out + (int64_t)blockIdx.y * a.Lout * a.inner;
+__device__ __forceinline__ void lines_write_zeros(const LineArgs& a, int64_t q0, int W, int64_t outer) {
+    float2* out = a.out + outer * a.Lout * a.inner;
     for (int i = threadIdx.x; i < a.Lout * W; i += blockDim.x) {
         const int o = i / W, w = i - o * W;
         if (q0 + w < a.inner) out[(int64_t)o * a.inner + q0 + w] = make_float2(0.f, 0.f);
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(256) k_line(LineArgs a) {
     float2* tws = sm + 2 * L * W;
     const int64_t q0 = (int64_t)blockIdx.x * W;
     if (lines_unoccupied(a, q0, W)) {
-        if (a.skip_zero) lines_write_zeros(a, q0, W);
+        if (a.skip_zero) lines_write_zeros(a, q0, W, blockIdx.y);
         return;
     }
     const int64_t outer = blockIdx.y;
@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(256) k_line_ct(LineArgs a) {
     float2* tws = sm + 2 * L * W;
     const int64_t q0 = (int64_t)blockIdx.x * W;
     if (lines_unoccupied(a, q0, W)) {
-        if (a.skip_zero) lines_write_zeros(a, q0, W);
+        if (a.skip_zero) lines_write_zeros(a, q0, W, blockIdx.y);
         return;
     }
     const int64_t outer = blockIdx.y;
@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(NT, line_min_ctas(NT, P))
     const int q0 = (int)blockIdx.x * W;
     const int outer = (int)blockIdx.y;
     if (lines_unoccupied(a, q0, W)) {                // before any barrier or copy: the CTA leaves whole
-        if (a.skip_zero) lines_write_zeros(a, q0, W);
+        if (a.skip_zero) lines_write_zeros(a, q0, W, blockIdx.y);
         return;
     }
     if (threadIdx.x == 0) mbar_init(&bar, 1);
