@@ -555,8 +555,9 @@ __global__ void __launch_bounds__(NT, line_min_ctas(NT, P))
 // the x-pass output of the same plane in place (other clusters touch other
 // (x, column) planes only).  No TMA multicast: every copy is between global
 // memory and the issuing CTA's own shared memory.
-// Measured on the 256 x 256 x 128 workload (96 columns, one B200): 17.5 ms
-// forward and 16.3 ms adjoint, against 7.7 and 7.5 ms for the separate passes.
+// Measured on the 256 x 256 x 128 workload (96 columns, one B200, three-pass y
+// transforms in both): 17.5 ms forward and 16.3 ms adjoint, against 7.7 and
+// 7.5 ms for the separate passes.
 // Each cluster walks its plane as one serial chain (TMA load, y transforms,
 // cluster barrier, ten gather / transform / store rounds) at two CTAs per SM,
 // so the HBM round trip it saves does not pay; plans run these kernels only
