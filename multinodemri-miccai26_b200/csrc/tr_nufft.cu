@@ -1962,9 +1962,13 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
     fa.ncol = n_img * C;
     fa.err = p->dev_err;
     fa.poll = p->poll_limit;
-    // TMA variant: one image row x kTmaXWidth coils per CTA
-    if (p->use_tma && ct && maps && C % kTmaXWidth == 0 && X % 16 == 0 && X <= 256 && img_stride % 2 == 0 &&
-        (int64_t)X * (kTmaXWidth + 1) <= (int64_t)OSX * kTmaXWidth && OSX / 2 <= 256) {
+    // TMA variant: one image row x wt coils per CTA (8, or 4 where 8 does not divide C;
+    // the second output box then starts (OSX / 2) 32 bytes into the tile: 128-byte aligned
+    // when OSX % 8 == 0)
+    int wt = C % kTmaXWidth == 0 ? kTmaXWidth : (C % 4 == 0 ? 4 : 0);
+    if (wt == 4 && ((int64_t)(OSX / 2) * wt * 8) % 128) wt = 0;
+    if (p->use_tma && ct && maps && wt && X % 16 == 0 && X <= 256 && img_stride % 2 == 0 &&
+        (int64_t)X * (wt + 1) <= (int64_t)OSX * wt && OSX / 2 <= 256) {
         CUtensorMap timg, tmap, tout;
         const uint64_t nrows = (uint64_t)Z * Y;
         PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
@@ -1978,22 +1982,28 @@ static tr_status stage_fwd_x(tr_plan* p, const float2* images, int64_t img_strid
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
         }
-        ok = ok && encode_map_3d(&tmap, maps, (uint64_t)C, (uint64_t)X, nrows, (uint32_t)kTmaXWidth, (uint32_t)X);
-        ok = ok && encode_map_3d(&tout, p->bufA, (uint64_t)fa.ncol, (uint64_t)OSX, nrows, (uint32_t)kTmaXWidth,
+        ok = ok && encode_map_3d(&tmap, maps, (uint64_t)C, (uint64_t)X, nrows, (uint32_t)wt, (uint32_t)X);
+        ok = ok && encode_map_3d(&tout, p->bufA, (uint64_t)fa.ncol, (uint64_t)OSX, nrows, (uint32_t)wt,
                                  (uint32_t)(OSX / 2));
         const void* tfn = nullptr;
         unsigned nt = 256;
+        if (wt == kTmaXWidth) {
 #define TR_FWDX_TMA(LV) case LV: tfn = (const void*)k_fwd_x_tma<LV, kTmaXWidth>; break;
-        switch (OSX) { TR_CT_LENGTHS(TR_FWDX_TMA) default: break; }
+            switch (OSX) { TR_CT_LENGTHS(TR_FWDX_TMA) default: break; }
 #undef TR_FWDX_TMA
-        if (OSX == 320 && p->two_pass_320) {
-            tfn = (const void*)k_fwd_x_wide<320, kTmaXWidth>;
-            nt = kWideNT;
+            if (OSX == 320 && p->two_pass_320) {
+                tfn = (const void*)k_fwd_x_wide<320, kTmaXWidth>;
+                nt = kWideNT;
+            }
+        } else {
+#define TR_FWDX_TMA4(LV) case LV: tfn = (const void*)k_fwd_x_tma<LV, 4>; break;
+            switch (OSX) { TR_CT_LENGTHS(TR_FWDX_TMA4) default: break; }
+#undef TR_FWDX_TMA4
         }
         if (ok && tfn) {
-            const size_t smem = fft_smem_bytes(OSX, kTmaXWidth) + 128;
+            const size_t smem = fft_smem_bytes(OSX, wt) + 128;
             TR_TRY(set_smem_limit(tfn, smem));
-            dim3 grid((unsigned)(nrows * n_img), 1u, (unsigned)(C / kTmaXWidth));
+            dim3 grid((unsigned)(nrows * n_img), 1u, (unsigned)(C / wt));
             void* args[] = {&fa, &timg, &tmap, &tout};
             TR_CUDA(cudaLaunchKernel(tfn, grid, dim3(nt), args, smem, st));
             return TR_OK;
@@ -2304,21 +2314,30 @@ static tr_status stage_adj_x(tr_plan* p, int n_img, const float2* maps, int C, f
     aa.accumulate = 0;
     aa.err = p->dev_err;
     aa.poll = p->poll_limit;
-    // TMA variant: one image row per CTA, coil groups of kTmaXWidth
-    if (p->use_tma && ct && maps && C % kTmaXWidth == 0 && OSX / 2 <= 256 && X <= 256 && X + 4 <= OSX) {
+    // TMA variant: one image row per CTA, coil groups of wt (8, or 4 where 8 does not divide C
+    // and the second input box, (OSX / 2) 32-byte rows into the tile, is 128-byte aligned)
+    int wt = C % kTmaXWidth == 0 ? kTmaXWidth : (C % 4 == 0 ? 4 : 0);
+    if (wt == 4 && ((int64_t)(OSX / 2) * wt * 8) % 128) wt = 0;
+    if (p->use_tma && ct && maps && wt && OSX / 2 <= 256 && X <= 256 && X + 4 <= OSX) {
         CUtensorMap tin;
         const void* tfn = nullptr;
+        unsigned nt = (unsigned)ct_threads(OSX, wt);
+        if (wt == kTmaXWidth) {
 #define TR_ADJX_TMA(LV) case LV: tfn = (const void*)k_adj_x_tma<LV, kTmaXWidth>; break;
-        switch (OSX) { TR_CT_LENGTHS(TR_ADJX_TMA) default: break; }
+            switch (OSX) { TR_CT_LENGTHS(TR_ADJX_TMA) default: break; }
 #undef TR_ADJX_TMA
-        unsigned nt = (unsigned)ct_threads(OSX, kTmaXWidth);
-        if (OSX == 320 && p->two_pass_320 && X % 16 == 0) {  // X <= 256: kWideXBlocks blocks of 16 per warp
-            tfn = (const void*)k_adj_x_wide<320, kTmaXWidth>;
-            nt = kWideNT;
+            if (OSX == 320 && p->two_pass_320 && X % 16 == 0) {  // X <= 256: kWideXBlocks blocks of 16 per warp
+                tfn = (const void*)k_adj_x_wide<320, kTmaXWidth>;
+                nt = kWideNT;
+            }
+        } else {
+#define TR_ADJX_TMA4(LV) case LV: tfn = (const void*)k_adj_x_tma<LV, 4>; break;
+            switch (OSX) { TR_CT_LENGTHS(TR_ADJX_TMA4) default: break; }
+#undef TR_ADJX_TMA4
         }
-        if (tfn && encode_map_3d(&tin, p->bufA, (uint64_t)aa.ncol, (uint64_t)OSX, (uint64_t)Z * Y, (uint32_t)kTmaXWidth,
+        if (tfn && encode_map_3d(&tin, p->bufA, (uint64_t)aa.ncol, (uint64_t)OSX, (uint64_t)Z * Y, (uint32_t)wt,
                                  (uint32_t)(OSX / 2))) {
-            const size_t smem = fft_smem_bytes(OSX, kTmaXWidth) + 128;
+            const size_t smem = fft_smem_bytes(OSX, wt) + 128;
             TR_TRY(set_smem_limit(tfn, smem));
             dim3 grid((unsigned)((int64_t)Z * Y * n_img));
             void* args[] = {&aa, &tin};
