@@ -1517,11 +1517,16 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : (CG >= 4 ? 4 : 5))) k_spre
     const int tid = threadIdx.x;
     const int cst = a.cchunk;                                            // row stride of dq
 
-    if ((int)blockIdx.x >= a.n_work) {
+    // the zero-fill CTAs are spread evenly among the work items (CTA b is zero-fill
+    // group floor(b nz / T) when that floor steps at b), so store-only CTAs share
+    // the SMs with gathering ones instead of running as a tail
+    const int zper = TMA ? kZeroTilesTma : kZeroTiles;
+    const long long nzc = (a.n_empty + zper - 1) / zper, T = a.n_work + nzc, bb = blockIdx.x;
+    const long long zlo = bb * nzc / T, zhi = (bb + 1) * nzc / T;
+    if (zhi > zlo) {
         // ---- zero fill of tiles that no sample reaches (all columns, chunk 0 only)
         if (blockIdx.y != 0) return;
-        const int zper = TMA ? kZeroTilesTma : kZeroTiles;
-        const int z0 = ((int)blockIdx.x - a.n_work) * zper;
+        const int z0 = (int)zlo * zper;
         if constexpr (TMA) {
             float4* z4 = reinterpret_cast<float4*>(dq);          // one zero piece [kSpreadSub][cchunk]
             for (int i = tid; i < (kSpreadSub / 2) * cst; i += 256) z4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1560,7 +1565,7 @@ __global__ void __launch_bounds__(256, (CG >= 6 ? 3 : (CG >= 4 ? 4 : 5))) k_spre
 
     const int col0 = blockIdx.y * a.cchunk;
     const int ncc = min(a.cchunk, a.ncol - col0);
-    const int4 item = a.work[blockIdx.x];
+    const int4 item = a.work[bb - zlo];
     const int tile = item.x, beg = item.y, end = item.z, slot = item.w;
     int t0z, t0y, t0x, Tz, Ty, Tx;
     tile_geometry(a, tile, t0z, t0y, t0x, Tz, Ty, Tx);
