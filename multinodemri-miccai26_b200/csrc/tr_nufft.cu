@@ -2385,7 +2385,7 @@ tr_status nufft_forward_cols(tr_plan* p, int bin, const float2* images, int64_t 
 
 // Launch-shape autotuning (TR_PLAN_AUTOTUNE).  The first gridding of a column
 // count, outside stream capture, times k_spread for each candidate column chunk
-// on the caller's bin (CUDA events, best of two launches after one warm-up) and
+// on the caller's bin (CUDA events, the fastest of three launches after one warm-up) and
 // keeps the fastest for that column count.  The choice cannot change results:
 // every grid point sums its list in the same order whatever the chunking.
 static tr_status tune_spread_cols(tr_plan* p, int bin, const float2* ksp, int ncol, bool use_dcf, cudaStream_t st) {
@@ -2413,12 +2413,19 @@ static tr_status tune_spread_cols(tr_plan* p, int bin, const float2* ksp, int nc
         p->spread_cols = cols;
         rc = stage_spread(p, bin, ksp, ncol, use_dcf, st);
         if (rc != TR_OK) break;
-        cudaEventRecord(e0, st);
-        for (int r = 0; r < 2 && rc == TR_OK; ++r) rc = stage_spread(p, bin, ksp, ncol, use_dcf, st);
-        cudaEventRecord(e1, st);
-        if (rc != TR_OK || cudaEventSynchronize(e1) != cudaSuccess) break;
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
+        // the best of three launches timed one by one (two back to back flipped
+        // between close candidates from run to run)
+        float ms = 1e30f;
+        for (int r = 0; r < 3 && rc == TR_OK; ++r) {
+            cudaEventRecord(e0, st);
+            rc = stage_spread(p, bin, ksp, ncol, use_dcf, st);
+            cudaEventRecord(e1, st);
+            if (rc != TR_OK || cudaEventSynchronize(e1) != cudaSuccess) break;
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            ms = std::min(ms, t);
+        }
+        if (rc != TR_OK) break;
         if (ms < best) {
             best = ms;
             best_cols = cols;
